@@ -1,0 +1,224 @@
+"""ctypes binding of libqubo_b200.so (the C ABI in include/qubo_b200.h).
+
+The library must be built in-tree (``python __graft_entry__.py`` or ``build.py`` beside
+this file).  Importing the binding without it raises ImportError: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqubo_b200.so")
+
+QB_OK, QB_EINVAL, QB_ERANGE, QB_ENOMEM, QB_ECUDA, QB_ETIMEOUT, QB_ENODEV, QB_EOVERFLOW = range(8)
+QB_F32, QB_F64, QB_I8, QB_I16, QB_I32, QB_I64 = 1, 2, 3, 4, 5, 6
+FORMS = {"auto": 0, "gray": 1, "tc": 2, "exact": 3}
+FORM_NAMES = {v: k for k, v in FORMS.items()}
+TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
+
+_DTYPES = {
+    np.dtype(np.float32): QB_F32,
+    np.dtype(np.float64): QB_F64,
+    np.dtype(np.int8): QB_I8,
+    np.dtype(np.int16): QB_I16,
+    np.dtype(np.int32): QB_I32,
+    np.dtype(np.int64): QB_I64,
+}
+
+
+class QbProblem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int32), ("dtype", ctypes.c_int32), ("q", ctypes.c_void_p), ("ldq", ctypes.c_int64),
+                ("q_on_device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class QbOptions(ctypes.Structure):
+    _fields_ = [("form", ctypes.c_int32), ("tie_rule", ctypes.c_int32), ("fixed_bits", ctypes.c_int32),
+                ("prefix_bits", ctypes.c_int32), ("shard_index", ctypes.c_int32), ("shard_count", ctypes.c_int32),
+                ("max_candidates", ctypes.c_int32), ("flags", ctypes.c_int32), ("stream", ctypes.c_void_p)]
+
+
+class QbResult(ctypes.Structure):
+    _fields_ = [("best_x", ctypes.c_uint64), ("best_e", ctypes.c_double), ("best_e_int", ctypes.c_int64),
+                ("order_key", ctypes.c_uint64), ("pass1_min", ctypes.c_double), ("err_bound", ctypes.c_double),
+                ("states", ctypes.c_int64), ("candidate_records", ctypes.c_int64), ("form_used", ctypes.c_int32),
+                ("is_integer", ctypes.c_int32), ("found", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("pass1_ms", ctypes.c_float), ("pass2_ms", ctypes.c_float), ("kernels", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class QbError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where}: {strerror(status)} (status {status})")
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libqubo_b200.so (raises ImportError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build the CUDA library first (python __graft_entry__.py)")
+    L = ctypes.CDLL(LIB_PATH)
+    H = ctypes.c_void_p
+    L.qb_version.restype = ctypes.c_int
+    L.qb_strerror.argtypes = [ctypes.c_int]
+    L.qb_strerror.restype = ctypes.c_char_p
+    L.qb_handle_create.argtypes = [ctypes.c_int, ctypes.POINTER(H)]
+    L.qb_handle_destroy.argtypes = [H]
+    for name in ("qb_solve",):
+        getattr(L, name).argtypes = [H, ctypes.POINTER(QbProblem), ctypes.POINTER(QbOptions), ctypes.POINTER(QbResult)]
+    L.qb_solve_begin.argtypes = [H, ctypes.POINTER(QbProblem), ctypes.POINTER(QbOptions),
+                                 ctypes.POINTER(ctypes.c_double)]
+    L.qb_solve_finish.argtypes = [H, ctypes.c_double, ctypes.POINTER(QbResult)]
+    L.qb_solve_batch.argtypes = [H, ctypes.POINTER(QbProblem), ctypes.c_int32, ctypes.POINTER(QbOptions),
+                                 ctypes.POINTER(QbResult)]
+    L.qb_autotune.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    _lib = L
+    return L
+
+
+def strerror(status: int) -> str:
+    try:
+        return load().qb_strerror(int(status)).decode()
+    except ImportError:
+        return f"status {status}"
+
+
+def _raise(status: int, where: str):
+    if status == QB_EINVAL:
+        raise ValueError(f"{where}: {strerror(status)}")
+    if status == QB_ERANGE:
+        raise OverflowError(f"{where}: {strerror(status)}")
+    raise QbError(status, where)
+
+
+class Handle:
+    """One library handle (device stream + scratch).  Not shared between threads."""
+
+    def __init__(self, device: int):
+        L = load()
+        self.device = device
+        self._h = ctypes.c_void_p()
+        rc = L.qb_handle_create(int(device), ctypes.byref(self._h))
+        if rc:
+            _raise(rc, f"qb_handle_create(device={device})")
+
+    def close(self):
+        if self._h:
+            load().qb_handle_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    @staticmethod
+    def _problem(Q: np.ndarray) -> tuple[QbProblem, np.ndarray]:
+        Q = np.ascontiguousarray(Q)
+        if Q.ndim != 2 or Q.shape[0] != Q.shape[1]:
+            raise ValueError(f"Q must be square, got shape {Q.shape}")
+        if Q.dtype not in _DTYPES:
+            raise TypeError(f"unsupported Q dtype {Q.dtype}")
+        p = QbProblem(n=Q.shape[0], dtype=_DTYPES[Q.dtype], q=Q.ctypes.data, ldq=Q.shape[0], q_on_device=0)
+        return p, Q
+
+    @staticmethod
+    def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
+                max_candidates=0, stream=None) -> QbOptions:
+        return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
+                         prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
+                         max_candidates=int(max_candidates), flags=0, stream=stream)
+
+    def solve(self, Q: np.ndarray, **opts) -> dict:
+        p, keep = self._problem(Q)
+        o = self.options(**opts)
+        r = QbResult()
+        rc = load().qb_solve(self._h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(r))
+        del keep
+        if rc:
+            _raise(rc, "qb_solve")
+        return result_dict(r, p.n)
+
+    def solve_begin(self, Q: np.ndarray, **opts) -> float:
+        p, keep = self._problem(Q)
+        o = self.options(**opts)
+        v = ctypes.c_double()
+        rc = load().qb_solve_begin(self._h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(v))
+        del keep
+        if rc:
+            _raise(rc, "qb_solve_begin")
+        return v.value
+
+    def solve_finish(self, global_min: float, n: int) -> dict:
+        r = QbResult()
+        rc = load().qb_solve_finish(self._h, ctypes.c_double(global_min), ctypes.byref(r))
+        if rc:
+            _raise(rc, "qb_solve_finish")
+        return result_dict(r, n)
+
+    def solve_batch(self, Qs: list, **opts) -> list[dict]:
+        probs = (QbProblem * len(Qs))()
+        keep = []
+        for i, Q in enumerate(Qs):
+            p, k = self._problem(Q)
+            probs[i] = p
+            keep.append(k)
+        o = self.options(**opts)
+        res = (QbResult * len(Qs))()
+        rc = load().qb_solve_batch(self._h, probs, len(Qs), ctypes.byref(o), res)
+        if rc:
+            _raise(rc, "qb_solve_batch")
+        return [result_dict(res[i], probs[i].n) for i in range(len(Qs))]
+
+    def autotune(self, n: int, dtype) -> str:
+        f = ctypes.c_int32()
+        rc = load().qb_autotune(self._h, int(n), _DTYPES[np.dtype(dtype)], ctypes.byref(f))
+        if rc:
+            _raise(rc, "qb_autotune")
+        return FORM_NAMES[f.value]
+
+
+def result_dict(r: QbResult, n: int) -> dict:
+    x = int(r.best_x)
+    return {
+        "found": bool(r.found),
+        "best_X_int": x,
+        "best_X": np.array([(x >> (n - 1 - i)) & 1 for i in range(n)], dtype=np.int32),
+        "best_E": float(r.best_e),
+        "best_E_int": int(r.best_e_int),
+        "order_key": int(r.order_key),
+        "pass1_min": float(r.pass1_min),
+        "err_bound": float(r.err_bound),
+        "states": int(r.states),
+        "candidate_records": int(r.candidate_records),
+        "form": FORM_NAMES.get(int(r.form_used), str(r.form_used)),
+        "is_integer": bool(r.is_integer),
+        "pass1_ms": float(r.pass1_ms),
+        "pass2_ms": float(r.pass2_ms),
+        "kernels": int(r.kernels),
+    }
+
+
+_handles: dict[tuple[int, int], Handle] = {}
+
+
+def handle(device: int = 0) -> Handle:
+    """The calling thread's handle on `device` (created on first use)."""
+    key = (int(device), threading.get_ident())
+    with _lock:
+        h = _handles.get(key)
+        if h is None:
+            h = Handle(device)
+            _handles[key] = h
+        return h

@@ -1,0 +1,52 @@
+"""Build libqubo_b200.so in-tree for sm_100a (nvcc cross-compiles without a GPU).
+
+    python evo-quantum-qubolib_b200/build.py [--force] [--debug]
+
+--debug adds -DQB_CHECK (bounds checks that record a bad index and skip the access).
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libqubo_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-Xcompiler", "-fPIC",
+         "-shared", "-Xptxas", "-v"]
+
+
+def sources():
+    return [os.path.join(CSRC, "qb_capi.cu")]
+
+
+def deps():
+    return glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) + [
+        os.path.join(HERE, "..", "include", "qubo_b200.h")]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(OUT):
+        return False
+    t = os.path.getmtime(OUT)
+    return all(os.path.getmtime(d) <= t for d in deps())
+
+
+def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
+    if not force and not debug and up_to_date():
+        return OUT
+    cmd = [NVCC] + FLAGS + (["-DQB_CHECK"] if debug else []) + sources() + ["-o", OUT]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        sys.stderr.write(p.stdout + p.stderr)
+        raise RuntimeError("nvcc failed building libqubo_b200.so")
+    if verbose:
+        sys.stdout.write(p.stderr)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, debug="--debug" in sys.argv, verbose=True))

@@ -1,0 +1,629 @@
+// qb_capi.cu -- the C ABI of libqubo_b200.so (declared in include/qubo_b200.h) and the
+// host orchestration of one exhaustive search:
+//
+//   pass 1   a search-form kernel (tensor-core, Gray or exact) visits every state and
+//            writes one minimum per record of states;
+//   reduce   smallest record value (the pass-1 minimum);
+//   select   every record whose value is within 2 * err_bound of the global minimum;
+//   pass 2   exact (FP64 / integer) re-evaluation of the selected records with the tie
+//            rule's order key; the host takes the lexicographic minimum of (E, key).
+//
+// Only pass 1 touches all 2^n states.  For integer Q inside the fp32-exact range the
+// selection keeps exactly the records that hold a minimal state.
+#include "../../include/qubo_b200.h"
+#include "qb_common.cuh"
+#include "qb_exact.cuh"
+#include "qb_gray.cuh"
+#include "qb_reduce.cuh"
+#include "qb_tc.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct HostBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 4096);
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+constexpr double kTwo24 = 16777216.0;
+constexpr double kTwo53 = 9007199254740992.0;
+constexpr int kDefaultCap = 1 << 16;
+
+struct Plan {
+  int n = 0;
+  bool is_int = false;
+  double abs_sum = 0.0;
+  int form = QB_FORM_EXACT;
+  qb::RecGeom geom{};
+  qb::TieRule rule{};
+  double eps = 0.0;       // per-state error bound of pass-1 values
+  uint64_t rec_begin = 0; // this shard's records [rec_begin, rec_begin + rec_count)
+  uint64_t rec_count = 0;
+  uint64_t states = 0;
+  // Gray form
+  int a = 0, b = 0, ubits = 0;
+  uint64_t unit_begin = 0, unit_end = 0;
+  // TC form
+  qb::TcPlan tc{};
+};
+
+}  // namespace
+
+struct qb_handle_s {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t st = nullptr;
+  DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
+  HostBuf hW, hmisc, hout;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int sm_count = 0;
+  // state between qb_solve_begin and qb_solve_finish
+  bool pending = false;
+  Plan plan;
+  int kernels = 0;
+  float pass1_ms = 0.f;
+  double local_min = 0.0;
+  int64_t exact_count = 0;  // EXACT form: records evaluated in pass 1
+  int cap = kDefaultCap;
+  int autotuned_form[qb::kMaxN + 1] = {0};
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+  if (e == cudaErrorMemoryAllocation) return QB_ENOMEM;
+  return e == cudaSuccess ? QB_OK : QB_ECUDA;
+}
+
+#define QB_CUDA(expr)                          \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+
+int dtype_size(int dt) {
+  switch (dt) {
+    case QB_F32: return 4;
+    case QB_F64: return 8;
+    case QB_I8: return 1;
+    case QB_I16: return 2;
+    case QB_I32: return 4;
+    case QB_I64: return 8;
+    default: return 0;
+  }
+}
+
+double load_elem(const unsigned char* p, int dt) {
+  switch (dt) {
+    case QB_F32: { float v; memcpy(&v, p, 4); return v; }
+    case QB_F64: { double v; memcpy(&v, p, 8); return v; }
+    case QB_I8: { int8_t v; memcpy(&v, p, 1); return v; }
+    case QB_I16: { int16_t v; memcpy(&v, p, 2); return v; }
+    case QB_I32: { int32_t v; memcpy(&v, p, 4); return v; }
+    default: { int64_t v; memcpy(&v, p, 8); return (double)v; }
+  }
+}
+
+// Q (any dtype, host or device) -> W (n x n doubles) and sum |Q_ij|.
+int load_problem(qb_handle* h, const qb_problem* p, std::vector<double>& W, double* abs_sum, bool* is_int) {
+  const int n = p->n;
+  const int es = dtype_size(p->dtype);
+  std::vector<unsigned char> raw((size_t)n * n * es);
+  if (p->q_on_device) {
+    QB_CUDA(cudaMemcpy2DAsync(raw.data(), (size_t)n * es, p->q, (size_t)p->ldq * es, (size_t)n * es, n,
+                              cudaMemcpyDeviceToHost, h->st));
+    QB_CUDA(cudaStreamSynchronize(h->st));
+  } else {
+    const unsigned char* src = static_cast<const unsigned char*>(p->q);
+    for (int i = 0; i < n; ++i) memcpy(raw.data() + (size_t)i * n * es, src + (size_t)i * p->ldq * es, (size_t)n * es);
+  }
+  *is_int = p->dtype >= QB_I8;
+  W.assign((size_t)n * n, 0.0);
+  double s = 0.0;
+  std::vector<double> Q((size_t)n * n);
+  for (size_t i = 0; i < Q.size(); ++i) {
+    double v = load_elem(raw.data() + i * es, p->dtype);
+    if (!std::isfinite(v)) return QB_EINVAL;
+    Q[i] = v;
+    s += std::fabs(v);
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) W[(size_t)i * n + j] = (i == j) ? Q[(size_t)i * n + i] : Q[(size_t)i * n + j] + Q[(size_t)j * n + i];
+  *abs_sum = s;
+  return QB_OK;
+}
+
+int make_rule(const qb_options* o, int n, qb::TieRule* r) {
+  r->n = n;
+  r->kind = o->tie_rule;
+  r->k = r->A = r->B = 0;
+  if (o->tie_rule == QB_TIE_QBF) {
+    int k = o->fixed_bits;
+    if (k < 0 || k >= n + (n == 0)) return QB_EINVAL;
+    int m = n - k;
+    int A = o->prefix_bits;
+    if (A < 0) A = m - std::min(m, 20);
+    if (A > m) return QB_EINVAL;
+    r->k = k;
+    r->A = A;
+    r->B = m - A;
+  } else if (o->tie_rule == QB_TIE_QB_F1) {
+    int k = o->fixed_bits;
+    if (k < 0 || n - k < 19) return QB_EINVAL;
+    r->k = k;
+    r->A = n - k - 18;
+    r->B = 18;
+  } else if (o->tie_rule != QB_TIE_NATURAL) {
+    return QB_EINVAL;
+  }
+  return QB_OK;
+}
+
+void shard_range(uint64_t total, int idx, int cnt, uint64_t* b, uint64_t* e) {
+  // contiguous, as even as integer division allows
+  unsigned __int128 t = total;
+  *b = (uint64_t)(t * (unsigned)idx / (unsigned)cnt);
+  *e = (uint64_t)(t * (unsigned)(idx + 1) / (unsigned)cnt);
+}
+
+int choose_form(qb_handle* h, const Plan& P, int requested) {
+  if (requested == QB_FORM_EXACT) return QB_FORM_EXACT;
+  const bool tc_ok = qb::tc_supported(P.n);
+  if (requested == QB_FORM_TC) return tc_ok ? QB_FORM_TC : -1;
+  if (requested == QB_FORM_GRAY) return P.n >= 20 ? QB_FORM_GRAY : -1;
+  // auto
+  if (h->autotuned_form[P.n]) return h->autotuned_form[P.n];
+  if (tc_ok) return QB_FORM_TC;
+  if (P.n >= 20) return QB_FORM_GRAY;
+  return QB_FORM_EXACT;
+}
+
+int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
+  const int n = P.n;
+  const int shard_idx = o->shard_count > 1 ? o->shard_index : 0;
+  const int shard_cnt = o->shard_count > 1 ? o->shard_count : 1;
+  int form = choose_form(h, P, o->form);
+  if (form < 0) return QB_EINVAL;
+  P.form = form;
+  P.geom = qb::RecGeom{};
+  P.geom.n = n;
+  if (form == QB_FORM_EXACT) {
+    int f = std::min(n, 16);
+    P.geom.kind = qb::kGeomBlock;
+    P.geom.fbits = f;
+    uint64_t total = 1ull << (n - f);
+    uint64_t rb, re;
+    shard_range(total, shard_idx, shard_cnt, &rb, &re);
+    P.rec_begin = rb;
+    P.rec_count = re - rb;
+    P.states = P.rec_count << f;
+    P.eps = 0.0;
+    return QB_OK;
+  }
+  if (form == QB_FORM_GRAY) {
+    int b = std::max(13, n - 16);
+    int a = n - b;
+    int cbbits = b - 13;
+    int sbits = std::min(a, std::max(5, n - 34));
+    int ubits = std::max(7, std::max(sbits, std::min(a, a + cbbits - 11)));
+    ubits = std::min(ubits, a);
+    P.a = a;
+    P.b = b;
+    P.ubits = ubits;
+    P.geom.kind = qb::kGeomGray;
+    P.geom.a = a;
+    P.geom.b = b;
+    P.geom.sbits = sbits;
+    P.geom.cbbits = cbbits;
+    P.geom.gubits = ubits - sbits;
+    uint64_t units = 1ull << (a - ubits + cbbits);
+    shard_range(units, shard_idx, shard_cnt, &P.unit_begin, &P.unit_end);
+    P.rec_begin = P.unit_begin << (P.geom.gubits + 3);
+    P.rec_count = (P.unit_end - P.unit_begin) << (P.geom.gubits + 3);
+    P.states = (P.unit_end - P.unit_begin) << (ubits + 13);
+    P.eps = (P.is_int && P.abs_sum < kTwo24) ? 0.0 : qb::gray_error_bound(P.abs_sum);
+    return QB_OK;
+  }
+  // tensor-core form
+  qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc);
+  P.geom.kind = qb::kGeomTC;
+  P.geom.gl = P.tc.gl;
+  P.rec_begin = P.tc.rec_begin;
+  P.rec_count = P.tc.rec_count;
+  P.states = P.tc.states;
+  P.eps = P.tc.eps;
+  return QB_OK;
+}
+
+int upload_W(qb_handle* h, const std::vector<double>& W) {
+  size_t bytes = W.size() * sizeof(double);
+  QB_CUDA(h->hW.ensure(bytes));
+  QB_CUDA(h->W.ensure(bytes));
+  memcpy(h->hW.p, W.data(), bytes);
+  QB_CUDA(cudaMemcpyAsync(h->W.p, h->hW.p, bytes, cudaMemcpyHostToDevice, h->st));
+  return QB_OK;
+}
+
+int run_pass1(qb_handle* h, Plan& P) {
+  const qb::ProblemDev pd{P.n, static_cast<const double*>(h->W.p)};
+  if (P.form == QB_FORM_EXACT) {
+    QB_CUDA(h->exout.ensure(std::max<uint64_t>(P.rec_count, 1) * sizeof(qb::ExactOut)));
+    size_t sm = qb::exact_smem_bytes(P.n, P.geom.fbits);
+    QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    // chunked over the grid limit
+    const uint64_t maxg = 1u << 30;
+    for (uint64_t off = 0; off < P.rec_count; off += maxg) {
+      uint64_t g = std::min<uint64_t>(maxg, P.rec_count - off);
+      qb::exact_records_kernel<<<(unsigned)g, qb::kExactThreads, sm, h->st>>>(
+          pd, P.rule, P.geom, nullptr, nullptr, (int64_t)(P.rec_begin + P.rec_count), (int64_t)(P.rec_begin + off),
+          static_cast<qb::ExactOut*>(h->exout.p) + off);
+      ++h->kernels;
+    }
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+  }
+  QB_CUDA(h->rec.ensure(std::max<uint64_t>(P.rec_count, 1) * sizeof(float)));
+  if (P.form == QB_FORM_GRAY) {
+    QB_CUDA(h->gtab.ensure(((size_t)1 << P.a) * 32 * sizeof(float)));
+    size_t sm0 = qb::gray_gtab_smem(P.n, P.a);
+    QB_CUDA(cudaFuncSetAttribute(qb::gray_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm0));
+    unsigned gblocks = (unsigned)std::min<uint64_t>((1ull << P.a) / 8 + 1, (uint64_t)h->sm_count * 4);
+    qb::gray_gtab_kernel<<<gblocks, 256, sm0, h->st>>>(pd, P.a, P.b, static_cast<float*>(h->gtab.p));
+    ++h->kernels;
+    qb::GrayParams gp{};
+    gp.P = pd;
+    gp.a = P.a;
+    gp.b = P.b;
+    gp.cbbits = P.geom.cbbits;
+    gp.sbits = P.geom.sbits;
+    gp.gubits = P.geom.gubits;
+    gp.unit_begin = P.unit_begin;
+    gp.gtab = static_cast<const float*>(h->gtab.p);
+    gp.rec = static_cast<float*>(h->rec.p);
+    size_t sm = qb::gray_pass1_smem(P.n, P.a);
+    QB_CUDA(cudaFuncSetAttribute(qb::gray_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    uint64_t units = P.unit_end - P.unit_begin;
+    if (units) {
+      qb::gray_pass1_kernel<<<(unsigned)units, qb::kGrayThreads, sm, h->st>>>(gp);
+      ++h->kernels;
+    }
+    QB_CUDA(cudaGetLastError());
+    return QB_OK;
+  }
+  QB_CUDA(h->tcscratch.ensure(qb::tc_scratch_bytes(P.tc)));
+  int rc = qb::tc_launch(P.tc, pd, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st, h->sm_count, &h->kernels);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qb_version(void) { return 100; }
+
+const char* qb_strerror(int s) {
+  switch (s) {
+    case QB_OK: return "ok";
+    case QB_EINVAL: return "invalid argument";
+    case QB_ERANGE: return "Q magnitude out of the exact range (sum |Q| must be < 2^53)";
+    case QB_ENOMEM: return "device memory allocation failed";
+    case QB_ECUDA: return "CUDA runtime error";
+    case QB_ETIMEOUT: return "a bounded wait inside a kernel timed out";
+    case QB_ENODEV: return "no such CUDA device";
+    case QB_EOVERFLOW: return "too many candidate records";
+    default: return "unknown status";
+  }
+}
+
+int qb_handle_create(int device, qb_handle** out) {
+  if (!out) return QB_EINVAL;
+  *out = nullptr;
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt <= 0) {
+    cudaGetLastError();
+    return QB_ENODEV;
+  }
+  if (device < 0 || device >= cnt) return QB_ENODEV;
+  QB_CUDA(cudaSetDevice(device));
+  qb_handle* h = new qb_handle_s();
+  h->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
+  for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (e != cudaSuccess) {
+    qb_handle_destroy(h);
+    return cuda_fail(e);
+  }
+  h->st = h->own;
+  *out = h;
+  return QB_OK;
+}
+
+int qb_handle_destroy(qb_handle* h) {
+  if (!h) return QB_EINVAL;
+  cudaSetDevice(h->device);
+  if (h->own) cudaStreamSynchronize(h->own);
+  h->W.release();
+  h->gtab.release();
+  h->rec.release();
+  h->cand.release();
+  h->misc.release();
+  h->exout.release();
+  h->tcscratch.release();
+  h->hW.release();
+  h->hmisc.release();
+  h->hout.release();
+  for (auto& ev : h->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (h->own) cudaStreamDestroy(h->own);
+  delete h;
+  return QB_OK;
+}
+
+int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, double* local_min) {
+  if (!h || !p || !o || !local_min) return QB_EINVAL;
+  if (p->n < 1 || p->n > qb::kMaxN || !p->q || p->ldq < p->n || dtype_size(p->dtype) == 0) return QB_EINVAL;
+  if (o->shard_count > 1 && (o->shard_index < 0 || o->shard_index >= o->shard_count)) return QB_EINVAL;
+  QB_CUDA(cudaSetDevice(h->device));
+  h->st = o->stream ? static_cast<cudaStream_t>(o->stream) : h->own;
+  h->pending = false;
+  h->kernels = 0;
+  h->cap = o->max_candidates > 0 ? o->max_candidates : kDefaultCap;
+  Plan P;
+  P.n = p->n;
+  std::vector<double> W;
+  int rc = load_problem(h, p, W, &P.abs_sum, &P.is_int);
+  if (rc) return rc;
+  if (P.abs_sum >= kTwo53) return QB_ERANGE;
+  rc = make_rule(o, P.n, &P.rule);
+  if (rc) return rc;
+  rc = plan_problem(h, o, P);
+  if (rc) return rc;
+  rc = upload_W(h, W);
+  if (rc) return rc;
+  QB_CUDA(h->misc.ensure(64));
+  QB_CUDA(h->hmisc.ensure(64));
+  QB_CUDA(cudaEventRecord(h->ev[0], h->st));
+  rc = run_pass1(h, P);
+  if (rc) return rc;
+  double lmin = INFINITY;
+  if (P.form == QB_FORM_EXACT) {
+    QB_CUDA(cudaEventRecord(h->ev[1], h->st));
+    size_t bytes = P.rec_count * sizeof(qb::ExactOut);
+    QB_CUDA(h->hout.ensure(std::max<size_t>(bytes, 64)));
+    if (bytes) QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, bytes, cudaMemcpyDeviceToHost, h->st));
+    QB_CUDA(cudaStreamSynchronize(h->st));
+    const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
+    for (uint64_t i = 0; i < P.rec_count; ++i) lmin = std::min(lmin, eo[i].e);
+    h->exact_count = (int64_t)P.rec_count;
+  } else {
+    uint32_t* mk = static_cast<uint32_t*>(h->misc.p);
+    QB_CUDA(cudaMemsetAsync(mk, 0xff, sizeof(uint32_t), h->st));
+    if (P.rec_count) {
+      unsigned blocks = (unsigned)std::min<uint64_t>((P.rec_count + 255) / 256, (uint64_t)h->sm_count * 8);
+      qb::rec_min_kernel<<<blocks, 256, 0, h->st>>>(static_cast<const float*>(h->rec.p), (int64_t)P.rec_count, mk);
+      ++h->kernels;
+      QB_CUDA(cudaGetLastError());
+    }
+    QB_CUDA(cudaEventRecord(h->ev[1], h->st));
+    QB_CUDA(cudaMemcpyAsync(h->hmisc.p, mk, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st));
+    QB_CUDA(cudaStreamSynchronize(h->st));
+    if (P.form == QB_FORM_TC) {
+      int trc = qb::tc_check_error(h->tcscratch.p, h->st);
+      if (trc) return trc;
+    }
+    uint32_t key = *static_cast<uint32_t*>(h->hmisc.p);
+    lmin = (P.rec_count && key != 0xffffffffu) ? (double)qb::key2f(key) : INFINITY;
+  }
+  QB_CUDA(cudaEventElapsedTime(&h->pass1_ms, h->ev[0], h->ev[1]));
+  h->plan = P;
+  h->local_min = lmin;
+  h->pending = true;
+  *local_min = lmin;
+  return QB_OK;
+}
+
+namespace {
+
+// Exact re-evaluation of `count` candidate records listed in h->cand (device).
+int rescore(qb_handle* h, const Plan& P, const qb::TieRule& rule, const qb::RecGeom& geom, int count,
+            std::vector<qb::ExactOut>& out) {
+  out.clear();
+  if (count <= 0) return QB_OK;
+  int maxf = 0;
+  {
+    uint64_t b, f;
+    qb::record_states(geom, 0, &b, &f);
+    maxf = __builtin_popcountll(f & qb::mask64(P.n));
+  }
+  if (maxf > qb::kExactMaxFree) return QB_EINVAL;
+  const qb::ProblemDev pd{P.n, static_cast<const double*>(h->W.p)};
+  QB_CUDA(h->exout.ensure((size_t)count * sizeof(qb::ExactOut)));
+  size_t sm = qb::exact_smem_bytes(P.n, maxf);
+  QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  qb::exact_records_kernel<<<count, qb::kExactThreads, sm, h->st>>>(pd, rule, geom,
+                                                                     static_cast<const uint64_t*>(h->cand.p), nullptr,
+                                                                     count, 0, static_cast<qb::ExactOut*>(h->exout.p));
+  ++h->kernels;
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(h->hout.ensure((size_t)count * sizeof(qb::ExactOut)));
+  QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, (size_t)count * sizeof(qb::ExactOut), cudaMemcpyDeviceToHost, h->st));
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
+  out.assign(eo, eo + count);
+  return QB_OK;
+}
+
+bool lex_less_h(const qb::ExactOut& a, const qb::ExactOut& b) {
+  return a.e < b.e || (a.e == b.e && a.key < b.key);
+}
+
+// QB_F1 rule, final step: smallest 18-bit suffix of the winning prefix with E == e_star.
+int qbf1_row(qb_handle* h, const Plan& P, uint64_t X, double e_star, uint64_t* Xout) {
+  qb::RecGeom g{};
+  g.kind = qb::kGeomBlock;
+  g.n = P.n;
+  g.fbits = 18;
+  qb::TieRule nat{qb::kTieNatural, P.n, 0, 0, 0};
+  uint64_t rid = X >> 18;
+  QB_CUDA(h->cand.ensure(sizeof(uint64_t)));
+  QB_CUDA(cudaMemcpyAsync(h->cand.p, &rid, sizeof(uint64_t), cudaMemcpyHostToDevice, h->st));
+  std::vector<qb::ExactOut> o;
+  int rc = rescore(h, P, nat, g, 1, o);
+  if (rc) return rc;
+  if (o.empty() || o[0].e != e_star) return QB_ECUDA;
+  *Xout = o[0].x;
+  return QB_OK;
+}
+
+}  // namespace
+
+int qb_solve_finish(qb_handle* h, double global_min, qb_result* r) {
+  if (!h || !r) return QB_EINVAL;
+  if (!h->pending) return QB_EINVAL;
+  h->pending = false;
+  Plan& P = h->plan;
+  memset(r, 0, sizeof(*r));
+  r->form_used = P.form;
+  r->is_integer = P.is_int ? 1 : 0;
+  r->pass1_min = h->local_min;
+  r->err_bound = P.eps;
+  r->states = (int64_t)P.states;
+  r->pass1_ms = h->pass1_ms;
+  QB_CUDA(cudaSetDevice(h->device));
+  QB_CUDA(cudaEventRecord(h->ev[2], h->st));
+  qb::ExactOut best{INFINITY, ~0ull, 0};
+  bool found = false;
+  if (P.form == QB_FORM_EXACT) {
+    const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
+    for (int64_t i = 0; i < h->exact_count; ++i)
+      if (lex_less_h(eo[i], best)) best = eo[i];
+    found = h->exact_count > 0 && best.e == global_min;
+    r->candidate_records = 0;
+  } else if (P.is_int && P.eps == 0.0 && global_min >= 0.0) {
+    // E(0) = 0 is minimal and X = 0 has the smallest key under every rule
+    found = P.rec_begin == 0 && P.rec_count > 0;
+    best = qb::ExactOut{0.0, 0ull, 0ull};
+  } else {
+    double thr = global_min + 2.0 * P.eps;
+    if (P.eps > 0.0) thr += std::fabs(thr) * 1e-12;
+    int* cnt = reinterpret_cast<int*>(static_cast<char*>(h->misc.p) + 16);
+    int count = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      QB_CUDA(h->cand.ensure((size_t)h->cap * sizeof(uint64_t)));
+      QB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), h->st));
+      if (P.rec_count) {
+        unsigned blocks = (unsigned)std::min<uint64_t>((P.rec_count + 255) / 256, (uint64_t)h->sm_count * 8);
+        qb::rec_select_kernel<<<blocks, 256, 0, h->st>>>(static_cast<const float*>(h->rec.p), (int64_t)P.rec_count,
+                                                          (int64_t)P.rec_begin, thr, static_cast<uint64_t*>(h->cand.p),
+                                                          cnt, h->cap);
+        ++h->kernels;
+        QB_CUDA(cudaGetLastError());
+      }
+      QB_CUDA(cudaMemcpyAsync(h->hmisc.p, cnt, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+      QB_CUDA(cudaStreamSynchronize(h->st));
+      count = *static_cast<int*>(h->hmisc.p);
+      if (count <= h->cap) break;
+      if (count > (1 << 24)) return QB_EOVERFLOW;
+      h->cap = count;
+    }
+    if (count > h->cap) return QB_EOVERFLOW;
+    std::vector<qb::ExactOut> outs;
+    int rc = rescore(h, P, P.rule, P.geom, count, outs);
+    if (rc) return rc;
+    for (auto& e : outs)
+      if (lex_less_h(e, best)) best = e;
+    found = count > 0;
+    r->candidate_records = count;
+  }
+  if (found && P.rule.kind == qb::kTieQBF1 && best.x != 0) {
+    uint64_t X;
+    int rc = qbf1_row(h, P, best.x, best.e, &X);
+    if (rc) return rc;
+    best.x = X;
+  }
+  QB_CUDA(cudaEventRecord(h->ev[3], h->st));
+  QB_CUDA(cudaEventSynchronize(h->ev[3]));
+  float ms2 = 0.f;
+  QB_CUDA(cudaEventElapsedTime(&ms2, h->ev[2], h->ev[3]));
+  r->pass2_ms = ms2;
+  r->found = found ? 1 : 0;
+  r->best_x = best.x;
+  r->best_e = found ? best.e : INFINITY;
+  r->best_e_int = (found && P.is_int) ? (int64_t)llround(best.e) : 0;
+  r->order_key = best.key;
+  r->kernels = h->kernels;
+  r->status = QB_OK;
+  return QB_OK;
+}
+
+int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* r) {
+  if (!r) return QB_EINVAL;
+  double lmin = 0.0;
+  int rc = qb_solve_begin(h, p, o, &lmin);
+  if (rc) {
+    memset(r, 0, sizeof(*r));
+    r->status = rc;
+    return rc;
+  }
+  rc = qb_solve_finish(h, lmin, r);
+  if (rc) r->status = rc;
+  return rc;
+}
+
+int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, const qb_options* o, qb_result* r) {
+  if (!h || !problems || !o || !r || count < 0) return QB_EINVAL;
+  for (int32_t i = 0; i < count; ++i) {
+    int rc = qb_solve(h, &problems[i], o, &r[i]);
+    if (rc) return rc;
+  }
+  return QB_OK;
+}
+
+int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
+  if (!h || !form_out || n < 1 || n > qb::kMaxN || dtype_size(dtype) == 0) return QB_EINVAL;
+  *form_out = n >= 20 ? QB_FORM_GRAY : QB_FORM_EXACT;
+  return QB_OK;
+}
+
+}  // extern "C"

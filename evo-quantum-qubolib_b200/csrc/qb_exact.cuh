@@ -1,0 +1,173 @@
+// qb_exact.cuh -- exact enumeration of state records (the "pass 2" kernel).
+//
+// One CTA per record.  A record is a set of 2^f states: a base state with f free bits
+// (record_states in qb_common.cuh).  Threads split the free bits: the top bits select a
+// thread, the low L bits are walked in Gray order with an incremental energy update
+//   flip v:  E += (1 - 2 x_v) * (W_vv + h_v),   h_u += (1 - 2 x_v) * W_uv  (u free, u != v)
+// in FP64, which is exact for integer Q with sum|Q| < 2^53.  Each thread keeps the
+// lexicographic minimum of (E, tie key); the CTA reduces and writes one ExactOut per
+// record.  The winner's energy is re-evaluated from scratch so the reported value does not
+// carry the walk's rounding.
+#pragma once
+#include "qb_common.cuh"
+
+namespace qb {
+
+struct ExactOut {
+  double e;
+  uint64_t key;
+  uint64_t x;
+};
+
+constexpr int kExactThreads = 256;
+constexpr int kExactMaxFree = 40;
+
+__device__ __forceinline__ double energy_from_scratch(const double* __restrict__ Ws, int n, uint64_t X) {
+  double e = 0.0;
+  uint64_t rem = X & mask64(n);
+  while (rem) {
+    int p = 63 - __clzll(rem);  // highest set bit = lowest variable index
+    rem &= ~(1ull << p);
+    int i = n - 1 - p;
+    const double* row = Ws + i * n;
+    e += row[i];
+    uint64_t r2 = rem;  // variables after i
+    while (r2) {
+      int q = 63 - __clzll(r2);
+      r2 &= ~(1ull << q);
+      e += row[n - 1 - q];
+    }
+  }
+  return e;
+}
+
+__device__ __forceinline__ bool lex_less(double e1, uint64_t k1, double e2, uint64_t k2) {
+  return e1 < e2 || (e1 == e2 && k1 < k2);
+}
+
+// rec_ids: candidate record indices (nullptr: record = rec_offset + blockIdx.x).
+// count_ptr: number of valid entries (nullptr: count_static).
+__global__ void __launch_bounds__(kExactThreads)
+exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restrict__ rec_ids,
+                     const int* __restrict__ count_ptr, int64_t count_static, int64_t rec_offset,
+                     ExactOut* __restrict__ out) {
+  extern __shared__ double smem_d[];
+  const int n = P.n;
+  const int64_t slot = (int64_t)blockIdx.x + (rec_ids ? rec_offset : 0);
+  const int64_t count = count_ptr ? (int64_t)(*count_ptr) : count_static;
+  if (slot >= count) return;
+  const uint64_t rid = rec_ids ? rec_ids[slot] : (uint64_t)(rec_offset + blockIdx.x);
+
+  double* Ws = smem_d;                       // n*n
+  double* Wl = Ws + n * n;                   // L*L couplings among low free variables
+  __shared__ int pos[kExactMaxFree];         // free bit positions, ascending
+  __shared__ int nfree;
+  __shared__ double red_e[kExactThreads / 32];
+  __shared__ uint64_t red_k[kExactThreads / 32], red_x[kExactThreads / 32];
+
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) Ws[i] = P.W[i];
+  uint64_t base, fm;
+  record_states(G, rid, &base, &fm);
+  if (threadIdx.x == 0) {
+    int c = 0;
+    uint64_t m = fm & mask64(n);
+    while (m && c < kExactMaxFree) {
+      int b = __ffsll((long long)m) - 1;
+      pos[c++] = b;
+      m &= m - 1;
+    }
+    nfree = c;
+  }
+  __syncthreads();
+  const int f = nfree;
+  const int tb = f < 8 ? f : 8;  // thread-selecting bits
+  const int L = f - tb;          // bits walked per thread
+  for (int i = threadIdx.x; i < L * L; i += blockDim.x) {
+    int a = i / L, c = i % L;
+    Wl[i] = Ws[(n - 1 - pos[a]) * n + (n - 1 - pos[c])];
+  }
+  __syncthreads();
+
+  double best_e = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+  uint64_t best_k = ~0ull, best_x = 0;
+  const int t = threadIdx.x;
+  if (t < (1 << tb)) {
+    uint64_t X = base;
+    for (int j = 0; j < tb; ++j)
+      if ((t >> j) & 1) X |= 1ull << pos[L + j];
+    double e = energy_from_scratch(Ws, n, X);
+    double h[kExactMaxFree];
+    for (int j = 0; j < L; ++j) {
+      int v = n - 1 - pos[j];
+      double s = 0.0;
+      uint64_t rem = X & mask64(n);
+      while (rem) {
+        int q = __ffsll((long long)rem) - 1;
+        rem &= rem - 1;
+        int u = n - 1 - q;
+        if (u != v) s += Ws[v * n + u];
+      }
+      h[j] = s;
+    }
+    best_e = e;
+    best_k = tie_key(R, X);
+    best_x = X;
+    const uint64_t steps = 1ull << L;
+    for (uint64_t s = 1; s < steps; ++s) {
+      int j = __ffsll((long long)s) - 1;
+      uint64_t bit = 1ull << pos[j];
+      bool on = !(X & bit);
+      int v = n - 1 - pos[j];
+      double d = Ws[v * n + v] + h[j];
+      e = on ? e + d : e - d;
+      X ^= bit;
+      const double* wl = Wl + j * L;
+      for (int u = 0; u < L; ++u) {
+        if (u == j) continue;
+        h[u] = on ? h[u] + wl[u] : h[u] - wl[u];
+      }
+      if (e <= best_e) {
+        uint64_t k = tie_key(R, X);
+        if (lex_less(e, k, best_e, best_k)) {
+          best_e = e;
+          best_k = k;
+          best_x = X;
+        }
+      }
+    }
+    best_e = energy_from_scratch(Ws, n, best_x);
+  }
+  // CTA reduction of (e, key, x)
+  for (int off = 16; off; off >>= 1) {
+    double oe = __shfl_down_sync(0xffffffffu, best_e, off);
+    uint64_t ok = __shfl_down_sync(0xffffffffu, best_k, off);
+    uint64_t ox = __shfl_down_sync(0xffffffffu, best_x, off);
+    if (lex_less(oe, ok, best_e, best_k)) {
+      best_e = oe;
+      best_k = ok;
+      best_x = ox;
+    }
+  }
+  if ((t & 31) == 0) {
+    red_e[t >> 5] = best_e;
+    red_k[t >> 5] = best_k;
+    red_x[t >> 5] = best_x;
+  }
+  __syncthreads();
+  if (t == 0) {
+    for (int w = 1; w < kExactThreads / 32; ++w)
+      if (lex_less(red_e[w], red_k[w], best_e, best_k)) {
+        best_e = red_e[w];
+        best_k = red_k[w];
+        best_x = red_x[w];
+      }
+    out[slot] = ExactOut{best_e, best_k, best_x};
+  }
+}
+
+inline size_t exact_smem_bytes(int n, int f) {
+  int L = f > 8 ? f - 8 : 0;
+  return (size_t)(n * n + L * L) * sizeof(double);
+}
+
+}  // namespace qb

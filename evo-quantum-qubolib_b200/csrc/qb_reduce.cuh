@@ -1,0 +1,37 @@
+// qb_reduce.cuh -- reduction of pass-1 record minima and selection of candidate records.
+//
+// Pass 1 writes one float per record: the minimum pass-1 energy over the record's states.
+// rec_min_kernel finds the smallest record value (order-preserving uint32 keys, atomicMin).
+// rec_select_kernel lists every record whose value is <= global_min + slack, where slack is
+// twice the per-state error bound of pass-1 arithmetic (0 for the exact integer path), so
+// every record that can hold an exact minimiser is re-evaluated in pass 2.
+#pragma once
+#include "qb_common.cuh"
+
+namespace qb {
+
+__global__ void rec_min_kernel(const float* __restrict__ rec, int64_t count, uint32_t* __restrict__ min_key) {
+  uint32_t k = 0xffffffffu;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    uint32_t v = f2key(rec[i]);
+    k = v < k ? v : k;
+  }
+  k = __reduce_min_sync(0xffffffffu, k);
+  if ((threadIdx.x & 31) == 0 && k != 0xffffffffu) atomicMin(min_key, k);
+}
+
+// Candidate indices are rec_index_offset + i for the selected positions i.
+__global__ void rec_select_kernel(const float* __restrict__ rec, int64_t count, int64_t rec_index_offset,
+                                  double threshold, uint64_t* __restrict__ cand, int* __restrict__ cand_count,
+                                  int cap) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    if ((double)rec[i] <= threshold) {
+      int s = atomicAdd(cand_count, 1);
+      if (s < cap) cand[s] = (uint64_t)(rec_index_offset + i);
+    }
+  }
+}
+
+}  // namespace qb

@@ -1,0 +1,154 @@
+/*
+ * qubo_b200.h -- C ABI of libqubo_b200.so, the B200 (sm_100a) exhaustive QUBO search.
+ *
+ * The reference (cloud-ru-tech/evo-quantum-qubolib) has no native library: its solvers are
+ * Python classes whose hot loops call numpy/cupy.  Each entry point below replaces one of
+ * those Python call sites; the citation beside it names the reference code it stands in for.
+ * A binding adds nothing but pointers and sizes: no torch, numpy or CUDA-runtime types
+ * cross this boundary (streams are passed as void*).
+ *
+ * Problem: minimise E(x) = sum_ij Q_ij x_i x_j over x in {0,1}^n, Q the full (possibly
+ * asymmetric) n x n matrix.  States are reported as the MSB-first integer X of the state
+ * vector: variable i is bit (n-1-i), the convention of the reference's best_X printout.
+ *
+ * Ties between minimal states follow the reference's search order (tie_rule):
+ *   QB_TIE_QBF   : with fixed_bits = k and prefix_bits = A, the smallest
+ *                  (first k bits as an integer, inverse-Gray rank of the next A bits,
+ *                   remaining bits as an integer) -- QBF's prefix loop
+ *                  (src/qubo_lib/solvers/qbf.py:188-230, 395-412) under Parallel's bit
+ *                  fixing (src/qubo_lib/solvers/parallel.py:145-157, lowest task first).
+ *   QB_TIE_QB_F1 : QB_F1's kernel order (src/qubo_lib/solvers/qbf1.py:179-249, 253-264):
+ *                  lowest thread of the 256x64 grid, then earliest Gray prefix, then the
+ *                  smallest 18-bit suffix of that prefix.
+ *   QB_TIE_NATURAL: smallest X.
+ * Float Q: the answer is the FP64 argmin (energies re-evaluated in FP64 on the GPU).
+ *
+ * Errors are returned as int status codes; no exceptions or exits cross the ABI.
+ * Thread-compatible per handle: one handle per host thread / stream.
+ */
+#ifndef QUBO_B200_H
+#define QUBO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define QB_OK 0
+#define QB_EINVAL 1      /* bad argument (n, dtype, split, pointer) */
+#define QB_ERANGE 2      /* |Q| too large for exact evaluation (see qb_solve) */
+#define QB_ENOMEM 3      /* device allocation failed */
+#define QB_ECUDA 4       /* CUDA runtime error */
+#define QB_ETIMEOUT 5    /* a bounded wait inside a kernel gave up */
+#define QB_ENODEV 6      /* no CUDA device / bad device index */
+#define QB_EOVERFLOW 7   /* too many candidate records (raise QB_MAX_CANDIDATES) */
+
+/* element types of Q */
+#define QB_F32 1
+#define QB_F64 2
+#define QB_I8 3
+#define QB_I16 4
+#define QB_I32 5
+#define QB_I64 6
+
+/* search forms */
+#define QB_FORM_AUTO 0   /* tensor-core form when it applies, else Gray form, else exact */
+#define QB_FORM_GRAY 1   /* plain Gray-code SIMT kernel (fp32 or int32 arithmetic) */
+#define QB_FORM_TC 2     /* tcgen05 contraction form (f16 digits, fp32 accumulate) */
+#define QB_FORM_EXACT 3  /* FP64 / integer-exact enumeration (small n) */
+
+/* tie rules */
+#define QB_TIE_QBF 0
+#define QB_TIE_QB_F1 1
+#define QB_TIE_NATURAL 2
+
+typedef struct qb_handle_s qb_handle;
+
+typedef struct qb_problem {
+  int32_t n;            /* variables, 1..62 */
+  int32_t dtype;        /* QB_F32 .. QB_I64 */
+  const void* q;        /* n x n, row-major, leading dimension ldq elements */
+  int64_t ldq;
+  int32_t q_on_device;  /* 0: host memory; 1: device memory of the handle's device */
+  int32_t reserved;
+} qb_problem;
+
+typedef struct qb_options {
+  int32_t form;         /* QB_FORM_* */
+  int32_t tie_rule;     /* QB_TIE_* */
+  int32_t fixed_bits;   /* QB_TIE_QBF: k leading task bits (Parallel splits_cnt = 2^k) */
+  int32_t prefix_bits;  /* QB_TIE_QBF: A inverse-Gray ranked bits after them; -1 = QBF default */
+  int32_t shard_index;  /* multi-GPU: this rank's share of the search space ... */
+  int32_t shard_count;  /* ... out of shard_count equal shares (1 = everything) */
+  int32_t max_candidates; /* cap on candidate records re-scored per pass-2 launch (0 = default) */
+  int32_t flags;        /* reserved, 0 */
+  void* stream;         /* cudaStream_t to run on; NULL = the handle's own stream */
+} qb_options;
+
+typedef struct qb_result {
+  uint64_t best_x;        /* MSB-first state integer */
+  double best_e;          /* E(best_x) in FP64 (exact for integer Q) */
+  int64_t best_e_int;     /* exact energy for integer Q */
+  uint64_t order_key;     /* tie-rule key of best_x (smaller wins among equal energies) */
+  double pass1_min;       /* minimum seen by the pass-1 kernel (fp32 arithmetic) */
+  double err_bound;       /* bound on |pass-1 value - exact value| per state */
+  int64_t states;         /* states whose energy entered the minimum in this call */
+  int64_t candidate_records; /* records re-evaluated exactly in pass 2 */
+  int32_t form_used;      /* QB_FORM_* actually run */
+  int32_t is_integer;     /* Q had an integer dtype */
+  int32_t found;          /* 1 if this call's share holds a minimal state */
+  int32_t status;
+  float pass1_ms;         /* device time of pass 1 (CUDA events) */
+  float pass2_ms;         /* device time of reduction + candidate re-evaluation */
+  int32_t kernels;        /* kernel launches issued by this call */
+  int32_t reserved;
+} qb_result;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int qb_version(void);
+
+/* Human-readable text of a status code. */
+const char* qb_strerror(int status);
+
+/* Open a handle on CUDA device `device`.  The handle owns a stream and its device scratch
+ * (per-record minima, candidate lists), grown on demand and freed by qb_handle_destroy.
+ * Replaces SolverABC.init_gpu / parse_device_arg (src/qubo_lib/abc/solver_abc.py:62-84). */
+int qb_handle_create(int device, qb_handle** out);
+int qb_handle_destroy(qb_handle* h);
+
+/* Exhaustive minimum of one problem: pass 1 (GPU kernel over all states, per-record
+ * minima), pass 2 (exact re-evaluation of the records that can hold the minimum), tie rule.
+ * Replaces QBF.prepare + iterate_prefix_interval + pack_results
+ * (src/qubo_lib/solvers/qbf.py:72-103, 188-230, 328-360) and QB_F1.prepare + QB_F1_kernel +
+ * pack_results (src/qubo_lib/solvers/qbf1.py:86-133, 179-249, 253-289).  Blocks until the
+ * result is on the host.  Integer Q needs sum|Q_ij| < 2^53 (else QB_ERANGE). */
+int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* r);
+
+/* Two-phase form of qb_solve for sharded (multi-GPU) searches: qb_solve_begin runs pass 1
+ * over this shard and returns its minimum in *local_min; the caller reduces the minima over
+ * all shards (min) and passes the global value to qb_solve_finish, which re-evaluates this
+ * shard's candidate records and fills *r (r->found = 0 when the shard holds no minimiser).
+ * Replaces devices_scheduler + merge_bruteforcer_partial_solutions
+ * (src/qubo_lib/solvers/scheduler.py:5-45, src/qubo_lib/solvers/parallel.py:225-320). */
+int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, double* local_min);
+int qb_solve_finish(qb_handle* h, double global_min, qb_result* r);
+
+/* Many independent problems in one launch sequence (persistent kernel over all
+ * (problem, tile) work items).  Results in r[0..count).  Replaces a host loop of
+ * QBF().solve calls (src/qubo_lib/solvers/qbf.py:48-70). */
+int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, const qb_options* o,
+                   qb_result* r);
+
+/* Pick the fastest form for problems of n variables and dtype by timing candidate kernel
+ * configurations on the handle's device; the choice is cached in the handle and used by
+ * QB_FORM_AUTO.  *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond
+ * QBF.define_chunk_size (src/qubo_lib/solvers/qbf.py:429-466), which picks a split. */
+int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUBO_B200_H */

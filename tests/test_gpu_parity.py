@@ -1,0 +1,193 @@
+"""GPU parity: every search form against the oracle (which is pinned to the reference) on
+seeded inputs, golden fixtures and edge cases.  Integer Q: bit-exact argmin and energy.
+Float Q: the FP64 argmin, energy within 1e-9 relative of the oracle's FP64 value."""
+import numpy as np
+import pytest
+
+import oracle
+import qubo_b200  # noqa: F401
+from conftest import bits_to_int, dec_q, load_golden
+from qubo_b200 import _lib
+from qubo_b200.problems import Just_Q, ReducedProblem
+from qubo_b200.solvers import QBF, QB_F1, Parallel
+
+pytestmark = pytest.mark.gpu
+
+FLOAT_RTOL = 1e-9
+
+
+def _x_int(sol) -> int:
+    return bits_to_int("".join(map(str, sol.best_X)))
+
+
+def _forms(n):
+    f = ["exact", "auto"]
+    if n >= 20:
+        f.append("gray")
+    if n >= 16:
+        f.append("tc")
+    return f
+
+
+def _check(Q, sol, ref):
+    if np.issubdtype(Q.dtype, np.integer):
+        assert _x_int(sol) == ref["best_X_int"], (sol.search, ref)
+        assert int(sol.best_E) == ref["best_E"]
+    else:
+        assert _x_int(sol) == ref["best_X_int"], (sol.search, ref)
+        e64 = oracle.energy(Q, ref["best_X_int"])
+        assert abs(float(sol.best_E) - e64) <= FLOAT_RTOL * max(1.0, abs(e64))
+
+
+def _solve(Q, form, **kw):
+    try:
+        return QBF().solve(Just_Q(Q), device="cuda", form=form, **kw)
+    except ValueError as e:
+        if form == "tc" and "invalid argument" in str(e):
+            pytest.skip("tensor-core form not available for this size")
+        raise
+
+
+def _rand_cases():
+    rng = np.random.default_rng(11)
+    out = []
+    for n in (1, 2, 3, 7, 12, 16, 19, 20, 21, 24, 26):
+        for dt in (np.int8, np.int16, np.int32, np.int64, np.float32, np.float64):
+            if np.issubdtype(dt, np.integer):
+                hi = 3 if dt == np.int8 else 100
+                U = rng.integers(-hi, hi + 1, (n, n)).astype(dt)
+                Q = U if n % 2 else (np.triu(U) + np.triu(U, 1).T).astype(dt)
+            else:
+                Q = rng.standard_normal((n, n)).astype(dt)
+            out.append((f"{np.dtype(dt).name}_n{n}", Q))
+    return out
+
+
+RAND = _rand_cases()
+
+
+@pytest.mark.parametrize("name,Q", RAND, ids=[c[0] for c in RAND])
+def test_random_all_forms(cuda_ok, name, Q):
+    n = Q.shape[0]
+    ref = oracle.qbf_port(Q)
+    for form in _forms(n):
+        _check(Q, _solve(Q, form), ref)
+
+
+GOLD = [c for c in load_golden("qbf_small.json")["cases"] if "error" not in c]
+
+
+@pytest.mark.parametrize("case", GOLD, ids=[c["name"] for c in GOLD])
+def test_golden_qbf_cases(cuda_ok, case):
+    Q = dec_q(case["Q"])
+    n = Q.shape[0]
+    kw = case["kwargs"]
+    A = kw.get("A", n - kw["B"] if "B" in kw else n - min(n, 20))
+    ref = oracle.qbf_port(Q, A=A)
+    for form in _forms(n):
+        _check(Q, _solve(Q, form, **kw), ref)
+
+
+@pytest.mark.parametrize("A", [0, 3, 9, 17, 23])
+def test_tie_rule_follows_split(cuda_ok, A):
+    """Heavily tied problem (every optimum has many twins): the winner depends on A exactly
+    as in the reference's prefix loop."""
+    n = 24
+    rng = np.random.default_rng(5)
+    Q = np.zeros((n, n), np.int32)
+    for i in range(0, n, 2):  # pairs (i, i+1) with E = -1 when exactly one of them is set
+        Q[i, i] = -1
+        Q[i + 1, i + 1] = -1
+        Q[i, i + 1] = 2
+    Q[rng.integers(0, n), rng.integers(0, n)] += 0
+    ref = oracle.qbf_port(Q, A=A)
+    for form in _forms(n):
+        _check(Q, _solve(Q, form, A=A), ref)
+
+
+def test_zero_and_positive_matrices(cuda_ok):
+    for Q in (np.zeros((22, 22), np.int16), np.ones((21, 21), np.int32), np.eye(25, dtype=np.float32)):
+        for form in _forms(Q.shape[0]):
+            sol = _solve(Q, form)
+            assert _x_int(sol) == 0 and float(sol.best_E) == 0.0
+
+
+PAR = load_golden("parallel_small.json")["cases"]
+
+
+@pytest.mark.parametrize("case", PAR, ids=[c["name"] for c in PAR])
+def test_parallel_single_device(cuda_ok, case):
+    Q = dec_q(case["Q"])
+    k_splits = case["splits_cnt"]
+    kw = {k: v for k, v in case["kwargs"].items()}
+    ref = oracle.parallel_port(Q, k_splits, A_sub=kw.get("A", -1))
+    sol = Parallel(base_solver=QBF, splits_cnt=k_splits, devices=["cuda"]).solve(Just_Q(Q), **kw)
+    _check(Q, sol, ref)
+    assert sol.epochs_cnt == k_splits and sol.solver_class == "QBF"
+    if np.issubdtype(Q.dtype, np.integer):
+        assert float(sol.best_E) == case["best_E"]
+
+
+@pytest.mark.parametrize("n,seed", [(19, 0), (20, 1), (22, 2), (24, 3)])
+def test_qb_f1_order(cuda_ok, n, seed):
+    rng = np.random.default_rng(seed)
+    U = rng.integers(-3, 4, (n, n)).astype(np.int16)
+    Q = (np.triu(U) + np.triu(U, 1).T).astype(np.int16)
+    ref = oracle.qbf1_numpy(Q)
+    sol = QB_F1().solve(Just_Q(Q), device="cuda")
+    assert _x_int(sol) == ref["best_X_int"] and sol.best_E == ref["best_E"]
+    assert sol.solver_class == "QB_F1" and sol.epochs_cnt == 1 and isinstance(sol.best_E, int)
+
+
+def test_qb_f1_rejects_non_int16(cuda_ok):
+    with pytest.raises(TypeError):
+        QB_F1().solve(Just_Q(np.zeros((20, 20), np.int32)), device="cuda")
+
+
+def test_reduced_problem_prefix_energy(cuda_ok):
+    rng = np.random.default_rng(9)
+    U = rng.integers(-20, 21, (26, 26)).astype(np.int32)
+    base = Just_Q(U)
+    rp = ReducedProblem(base, np.array([1, 0, 1]))
+    sol = QBF().solve(rp, device="cuda")
+    Qr = rp.build_Q_matrix()
+    ref = oracle.qbf_port(Qr)
+    assert _x_int(sol) == ref["best_X_int"]
+    assert sol.prefix_E == rp.prefix_E
+
+
+def test_errors(cuda_ok):
+    Q = np.zeros((8, 8), np.int32)
+    with pytest.raises(ValueError):
+        QBF().solve(Just_Q(Q), device="cpu")
+    with pytest.raises(ValueError):
+        QBF().solve(Just_Q(Q), use_gpu=True)
+    with pytest.raises(ValueError):
+        QBF().solve(Just_Q(Q), device="cuda", A=9)
+    with pytest.raises(ValueError):
+        Parallel(base_solver=QBF, splits_cnt=3, devices=["cuda"])
+    with pytest.raises(ValueError):
+        Parallel(base_solver=QBF, splits_cnt=2, devices=["cpu", "cuda"])
+
+
+def test_c_abi_two_phase_matches_single_call(cuda_ok):
+    """qb_solve_begin / qb_solve_finish over 3 shards reproduce qb_solve."""
+    rng = np.random.default_rng(21)
+    U = rng.integers(-50, 51, (27, 27)).astype(np.int32)
+    Q = (np.triu(U) + np.triu(U, 1).T).astype(np.int32)
+    h = _lib.handle(0)
+    for form in ("gray", "exact", "auto"):
+        whole = h.solve(Q, form=form)
+        mins = []
+        for s in range(3):
+            mins.append(h.solve_begin(Q, form=form, shard_index=s, shard_count=3))
+            h.solve_finish(mins[-1], 27)
+        gmin = min(mins)
+        outs = []
+        for s in range(3):
+            h.solve_begin(Q, form=form, shard_index=s, shard_count=3)
+            outs.append(h.solve_finish(gmin, 27))
+        found = [o for o in outs if o["found"]]
+        best = min(found, key=lambda o: (o["best_E"], o["order_key"]))
+        assert best["best_X_int"] == whole["best_X_int"] and best["best_E"] == whole["best_E"]
+        assert sum(o["states"] for o in outs) == 2 ** 27
