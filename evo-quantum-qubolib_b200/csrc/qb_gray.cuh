@@ -43,9 +43,9 @@ inline double gray_error_bound(double abs_sum) { return 300.0 * abs_sum * 5.9604
 
 // G(p)[c] for every Gray step i: one warp per step, lane = c.
 __global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__ gtab) {
-  extern __shared__ double sm[];
+  extern __shared__ double gtab_smem[];
   const int n = P.n;
-  double* Ws = sm;             // n*n
+  double* Ws = gtab_smem;      // n*n
   double* beta = Ws + n * n;   // a * 32
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) Ws[i] = P.W[i];
   __syncthreads();

@@ -6,29 +6,41 @@
 //   u = X & 255          (8 bits: the 256 columns of an MMA tile)
 // and the energy as
 //   E(t, y, u) = R_t(y) + C_t(u) + y^T V u
-//   R_t(y) = energy of the (t, y) variables alone            (per row, per tile)
-//   C_t(u) = E_U(u) + (t^T W_TU) u                            (per column, per tile)
-//   V      = couplings between the y and u variables          (fixed)
+//   R_t(y) = E_T(t) + E_Y(y) + (t^T W_TY) y       (per row, per tile: added after the row min)
+//   C_t(u) = E_U(u) + (t^T W_TU) u                (per column, per tile: folded into the MMA)
+//   V      = couplings between the y and u variables (fixed)
 // One tcgen05.mma (kind::f16, M=128, N=256, K=16, fp32 accumulators in TMEM) computes
 // D[y][u] = y^T V u + C_t(u) for all 32768 states of a tile:
 //   A[y][2i+d] = y_i * s_d         B[u][2i+d] = digit_d((V u)_i)      i < 7, d in {0,1}
 //   A[y][14+d] = s_d               B[u][14+d] = digit_d(C_t(u))
 // with digits v = d0 + s_1 d1 (integer Q: s = (1, 2048), d0 in [0, 2048), exact in fp16;
 // float Q: s = (1, 1), d0 + d1 = fp16 hi/lo split of v).  A is constant; per tile only
-// the two C columns of B change.  The epilogue reads each row's 256 accumulators
-// (tcgen05.ld), takes the row minimum with 3-input fp32 min, adds R_t(y) and keeps the
-// running minimum; every 2^gl tiles each epilogue warp writes one record (32 rows x 128
-// columns x 2^gl tiles).
+// the two C columns of B change.  The epilogue reads the accumulators (tcgen05.ld), takes
+// row minima with 3-input fp32 min and adds R_t(y).
 //
-// Roles (one persistent CTA per SM, 384 threads):
-//   warp 0      tile walk: Gray update of t, per-tile row increment and C tables
+// Measured on B200 (sm_100a): one N=256 MMA per 32768 states, consumed through
+// tcgen05.commit / mbarrier, costs about 450 cycles of pipeline round trip, and smaller N
+// does not shorten it, so tiles use the largest N; the TMEM holds two 256-column
+// accumulator stages.  The fp32 min pipe (about 128 values per clock per SM, shared with
+// fp32 adds) bounds the epilogue at half the MMA rate.
+//
+// Roles (one persistent CTA per SM, 640 threads):
+//   warp 0      tile walk: 32 tiles per step, one per lane.  t = (t_hi, t_lo) with t_lo the
+//               5 low bits: per-CTA tables give the t_lo parts, t_hi (constant over an
+//               aligned run of 32 Gray tiles) is Gray-updated once per run; each lane
+//               publishes E_T(t), t^T W_TY and t^T W_TU of its tile
 //   warp 1      TMEM allocation and MMA issue (one elected thread)
-//   warps 2-3   B producers: C_t(u) digits into the B stage (generic stores + proxy fence)
-//   warps 4-11  epilogue: warp w reads TMEM lanes 32*(w%4).. and column half (w-4)/4
-// Pipelines: 8 tile-parameter slots, 4 B stages, 2 accumulator stages (2 x 256 TMEM
-// columns), all on mbarriers.  Every wait is bounded (%globaltimer): on timeout the
-// waiting role raises an error flag, the CTA drains and frees TMEM, and the host reports
-// QB_ETIMEOUT.
+//   warps 2-3   B producers, alternate tiles: C_t(u) digits into the B stage (generic
+//               stores + proxy fence)
+//   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4)..+31 and the column quarter
+//               64*((w-4)/4)..+63 of every tile; it releases the accumulator stage as soon
+//               as its loads have landed, then reduces
+// Pipelines on mbarriers: 64 tile-parameter slots, 8 B stages, 2 accumulator stages.
+// Every wait is bounded (%globaltimer): on timeout the waiting role raises an error flag,
+// the CTA drains and frees TMEM, and the host reports QB_ETIMEOUT.
+//
+// Records: every 2^gl tiles (gl >= 5) each epilogue warp writes the minimum over its 32
+// rows x 64 columns x 2^gl tiles.
 //
 // Integer Q with sum|Q| <= 2^22 is exact (all partial sums stay below 2^24 in fp32).
 // Otherwise every value is within tc_error_bound() of the exact energy.
@@ -40,10 +52,12 @@
 namespace qb {
 
 constexpr double kTcIntMaxAbsSum = 4194304.0;  // 2^22
-constexpr int kTcThreads = 384;
-constexpr int kTcParamSlots = 8;
-constexpr int kTcBStages = 4;
-constexpr int kTcMaxNT = kMaxN - 15;
+constexpr int kTcThreads = 640;
+constexpr int kTcStages = 2;                   // TMEM accumulator stages (2 x 256 columns)
+constexpr int kTcEpiWarps = 16;
+constexpr int kTcParamSlots = 64;
+constexpr int kTcBStages = 8;
+constexpr int kTcN = 256;                      // MMA N = tile columns
 constexpr uint64_t kTcWaitLimitNs = 2000000000ull;  // 2 s per wait
 
 struct TcPlan {
@@ -54,7 +68,6 @@ struct TcPlan {
   double eps = 0.0;        // per-state error bound, unscaled units
   uint64_t tile_begin = 0, tile_end = 0;  // this shard's Gray tile indices
   uint64_t rec_begin = 0, rec_count = 0, states = 0;
-  int ctas = 0;
 };
 
 struct TcParams {
@@ -63,13 +76,13 @@ struct TcParams {
   float inv_scale;
   const double* W;          // scaled W, n*n
   uint64_t tile_begin;      // shard start (aligned to 2^gl)
-  uint64_t groups;          // record groups in this shard
-  uint64_t groups_per_cta;  // contiguous groups per CTA (last CTA may have fewer)
-  float* rec;               // rec[0] = record (tile_begin >> gl) << 3
+  uint64_t groups;          // record blocks (2^gl tiles each) in this shard
+  uint64_t groups_per_cta;  // contiguous blocks per CTA (last CTA may have fewer)
+  float* rec;               // rec[0] = record (tile_begin >> gl) << 4
   unsigned* err;            // error word
 };
 
-inline bool tc_supported(int n) { return n >= 15 && n <= kMaxN; }
+inline bool tc_supported(int n) { return n >= 20 && n <= kMaxN; }
 
 // per-state error bound of the float-digit path (unscaled units)
 inline double tc_error_bound(double abs_sum) { return 256.0 * abs_sum * 5.9604644775390625e-08 + 1e-300; }
@@ -89,15 +102,15 @@ inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard
     p->scale = std::ldexp(1.0, e);
     p->eps = tc_error_bound(abs_sum);
   }
-  p->gl = std::max(0, std::min(p->nt, n - 15 - 19));  // at most 2^22 records
+  p->gl = std::max(5, p->nt - 18);  // runs of 32 tiles; at most 2^22 records (16 per block)
   uint64_t groups = 1ull << (p->nt - p->gl);
   unsigned __int128 g = groups;
   uint64_t gb = (uint64_t)(g * (unsigned)shard_idx / (unsigned)shard_cnt);
   uint64_t ge = (uint64_t)(g * (unsigned)(shard_idx + 1) / (unsigned)shard_cnt);
   p->tile_begin = gb << p->gl;
   p->tile_end = ge << p->gl;
-  p->rec_begin = gb << 3;
-  p->rec_count = (ge - gb) << 3;
+  p->rec_begin = gb << 4;
+  p->rec_count = (ge - gb) << 4;
   p->states = (p->tile_end - p->tile_begin) << 15;
 }
 
@@ -123,16 +136,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: the warp sleeps in hardware until the phase completes
+// (or the hint, in ns, runs out) instead of spinning on shared memory
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(1000000u)
+      : "memory");
+  return ok != 0;
+}
 // bounded wait: false on timeout (or when another role already gave up)
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
   if (mbar_try_wait(b, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
-  for (uint32_t it = 0;; ++it) {
-    if (mbar_try_wait(b, parity)) return true;
-    if ((it & 63) == 63) {
-      if (*abort_flag) return false;
-      if (globaltimer_ns() - t0 > kTcWaitLimitNs) return false;
-    }
+  for (;;) {
+    if (mbar_try_wait_sleep(b, parity)) return true;
+    if (*abort_flag) return false;
+    if (globaltimer_ns() - t0 > kTcWaitLimitNs) return false;
   }
 }
 
@@ -152,7 +174,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // instruction descriptor, kind::f16: A = B = f16, D = f32, both K-major, M = 128, N = 256
-constexpr uint32_t kTcIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kTcIdesc =
+    (1u << 4) | (0u << 7) | (0u << 10) | (((uint32_t)kTcN >> 3) << 17) | ((128u >> 4) << 24);
 
 __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc) {
   asm volatile(
@@ -177,6 +200,15 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
       : "r"(taddr))
 
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// tcgen05.ld writes its registers asynchronously; only tcgen05.wait::ld makes them valid.
+// Passing each register through an empty volatile asm after the wait gives every later use
+// a data dependence on a statement ordered after the wait, so the compiler cannot hoist a
+// use above it.
+__device__ __forceinline__ void reg_fence32(uint32_t* r) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) asm volatile("" : "+r"(r[i]));
+}
 
 __device__ __forceinline__ float min32(const uint32_t* r) {
   float m0 = fmin3(__uint_as_float(r[0]), __uint_as_float(r[1]), __uint_as_float(r[2]));
@@ -213,15 +245,16 @@ __device__ __forceinline__ __half2 digits(float v, int exact) {
   return __halves2half2(lo, hi);
 }
 
+// per-tile parameters published by the tile walk
 struct TcSlot {
-  float F[32];  // F[0..15]: C contribution of the low 4 u bits, F[16..31]: high 4 bits
-  double d;     // W_kk + field of the flipped tile variable before the flip
-  int k;        // flipped tile bit (-1: none)
-  float sgn;    // +1 when the bit turns on
+  float f[8];  // f_j = (t^T W_TU)_j: C_t(u) = E_U(u) + sum_j f_j u_j
+  float g[8];  // g_i = (t^T W_TY)_i, i < 7
+  float et;    // E_T(t)
+  float pad[3];
 };
 
 struct TcSmemLayout {
-  uint32_t a_off, b_off, bar_off, slot_off, eu_off, misc_off, hy_off, w_off, total;
+  uint32_t a_off, b_off, bar_off, slot_off, eu_off, misc_off, lo_off, w_off, total;
 };
 
 __host__ __device__ inline TcSmemLayout tc_layout(int n) {
@@ -230,17 +263,17 @@ __host__ __device__ inline TcSmemLayout tc_layout(int n) {
   L.a_off = o;
   o += 128 * 32;  // A: 128 rows x 16 f16
   L.b_off = o;
-  o += kTcBStages * 256 * 32;
+  o += kTcBStages * kTcN * 32;
   L.bar_off = o;
-  o += (2 * kTcParamSlots + 2 * kTcBStages + 4) * 8;
+  o += (2 * kTcParamSlots + 2 * kTcBStages + 2 * kTcStages) * 8;
   L.slot_off = o;
   o += kTcParamSlots * sizeof(TcSlot);
   L.eu_off = o;
-  o += 256 * 4;
+  o += kTcN * 4;
   L.misc_off = o;
   o += 64;
-  L.hy_off = o;
-  o += (uint32_t)(n - 15) * 128 * 8;
+  L.lo_off = o;
+  o += 32 * 16 * 8;  // per t_lo pattern: f (7), g (7), E_lo, pad -- fp64
   L.w_off = o;
   o += (uint32_t)n * n * 8;
   L.total = o;
@@ -248,50 +281,50 @@ __host__ __device__ inline TcSmemLayout tc_layout(int n) {
 }
 
 __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
-  extern __shared__ __align__(1024) unsigned char sm[];
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
   const int n = P.n, nt = P.nt;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const TcSmemLayout L = tc_layout(n);
-  unsigned char* Asm = sm + L.a_off;
-  unsigned char* Bsm = sm + L.b_off;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L.bar_off);
+  unsigned char* Asm = tc_smem + L.a_off;
+  unsigned char* Bsm = tc_smem + L.b_off;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + L.bar_off);
   uint64_t* p_full = bars;
   uint64_t* p_empty = p_full + kTcParamSlots;
   uint64_t* b_full = p_empty + kTcParamSlots;
   uint64_t* b_empty = b_full + kTcBStages;
   uint64_t* acc_full = b_empty + kTcBStages;
-  uint64_t* acc_empty = acc_full + 2;
-  TcSlot* slots = reinterpret_cast<TcSlot*>(sm + L.slot_off);
-  float* EU = reinterpret_cast<float*>(sm + L.eu_off);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L.misc_off);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L.misc_off + 4);
-  double* ET0 = reinterpret_cast<double*>(sm + L.misc_off + 8);
-  double* hY = reinterpret_cast<double*>(sm + L.hy_off);
-  double* Ws = reinterpret_cast<double*>(sm + L.w_off);
+  uint64_t* acc_empty = acc_full + kTcStages;
+  TcSlot* slots = reinterpret_cast<TcSlot*>(tc_smem + L.slot_off);
+  float* EU = reinterpret_cast<float*>(tc_smem + L.eu_off);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + L.misc_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tc_smem + L.misc_off + 4);
+  double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
+  double* Ws = reinterpret_cast<double*>(tc_smem + L.w_off);
 
-  // this CTA's record groups and tiles (Gray indices)
+  // this CTA's blocks of 2^gl tiles (Gray indices)
   const uint64_t g0 = (uint64_t)blockIdx.x * P.groups_per_cta;
   if (g0 >= P.groups) return;  // uniform per CTA
   const uint64_t g1 = min(P.groups, g0 + P.groups_per_cta);
   const uint64_t i_begin = P.tile_begin + (g0 << P.gl);
-  const uint64_t ntiles = (g1 - g0) << P.gl;
+  const uint64_t ntiles = (g1 - g0) << P.gl;  // a multiple of 32
   const uint64_t t0 = gray64(i_begin);
   const float s1 = P.exact ? 2048.0f : 1.0f;
+  // variables: t bit k <-> n-16-k, y bit i <-> n-9-i, u bit j <-> n-1-j
 
   // ---------------------------------------------------------------- set-up
   for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
       mbar_init(&p_full[s], 1);
-      mbar_init(&p_empty[s], 10);  // 2 producer warps + 8 epilogue warps
+      mbar_init(&p_empty[s], 1 + kTcEpiWarps);  // the tile's producer warp + every epilogue warp
     }
     for (int s = 0; s < kTcBStages; ++s) {
-      mbar_init(&b_full[s], 2);
+      mbar_init(&b_full[s], 1);
       mbar_init(&b_empty[s], 1);
     }
-    for (int s = 0; s < 2; ++s) {
+    for (int s = 0; s < kTcStages; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], 8);
+      mbar_init(&acc_empty[s], kTcEpiWarps);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -301,7 +334,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   __syncthreads();
-  // variables: t bit k <-> n-16-k, y bit i <-> n-9-i, u bit j <-> n-1-j
   // A operand (constant)
   for (int e = tid; e < 128 * 16; e += kTcThreads) {
     int y = e >> 4, k = e & 15;
@@ -313,7 +345,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
   }
   // B operand, coupling columns (same in every stage)
-  for (int e = tid; e < 256 * 7; e += kTcThreads) {
+  for (int e = tid; e < kTcN * 7; e += kTcThreads) {
     int u = e / 7, i = e % 7;
     const double* row = Ws + (n - 9 - i) * n;
     double v = 0.0;
@@ -321,10 +353,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       if ((u >> j) & 1) v += row[n - 1 - j];
     __half2 dg = digits((float)v, P.exact);
     for (int s = 0; s < kTcBStages; ++s)
-      *reinterpret_cast<__half2*>(Bsm + s * 256 * 32 + kmaj_off(u, 2 * i)) = dg;
+      *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
   }
   // E_U(u)
-  for (int u = tid; u < 256; u += kTcThreads) {
+  for (int u = tid; u < kTcN; u += kTcThreads) {
     double e = 0.0;
     for (int j = 0; j < 8; ++j) {
       if (!((u >> j) & 1)) continue;
@@ -335,25 +367,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     }
     EU[u] = (float)e;
   }
-  // hY[k][y] = sum_i y_i W(t var k, y var i)
-  for (int e = tid; e < nt * 128; e += kTcThreads) {
-    int k = e >> 7, y = e & 127;
-    const double* row = Ws + (n - 16 - k) * n;
+  // t_lo tables: LO[p*16 + j] = (p^T W_TlU)_j (j < 8), LO[p*16 + 8 + i] = (p^T W_TlY)_i
+  // (i < 7), LO[p*16 + 15] = energy of the t_lo bits p
+  for (int e = tid; e < 32 * 16; e += kTcThreads) {
+    const int p = e >> 4, c = e & 15;
     double v = 0.0;
-    for (int i = 0; i < 7; ++i)
-      if ((y >> i) & 1) v += row[n - 9 - i];
-    hY[e] = v;
-  }
-  if (tid == 0) {  // E_T(t0)
-    double e = 0.0;
-    for (int k = 0; k < nt; ++k) {
-      if (!((t0 >> k) & 1)) continue;
-      const double* row = Ws + (n - 16 - k) * n;
-      e += row[n - 16 - k];
-      for (int k2 = 0; k2 < k; ++k2)
-        if ((t0 >> k2) & 1) e += row[n - 16 - k2];
+    if (c == 15) {
+      for (int k = 0; k < 5; ++k) {
+        if (!((p >> k) & 1)) continue;
+        const double* row = Ws + (n - 16 - k) * n;
+        v += row[n - 16 - k];
+        for (int k2 = 0; k2 < k; ++k2)
+          if ((p >> k2) & 1) v += row[n - 16 - k2];
+      }
+    } else {
+      const int col = c < 8 ? n - 1 - c : n - 9 - (c - 8);
+      for (int k = 0; k < 5; ++k)
+        if ((p >> k) & 1) v += Ws[(n - 16 - k) * n + col];
     }
-    *ET0 = e;
+    LO[e] = v;
   }
   fence_proxy_async();  // A / B stores (generic proxy) -> visible to tcgen05.mma
   tc_fence_before();
@@ -364,53 +396,70 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   bool ok = true;
   if (warp == 0) {
     // ---------------------------------------------------------- tile walk
-    double h0 = 0.0, h1 = 0.0, f = 0.0;  // fields of t bits lane, lane+32; f_lane (lane < 8)
-    const int m0 = lane, m1 = lane + 32;
-    for (int k = 0; k < nt; ++k) {
-      if (!((t0 >> k) & 1)) continue;
-      const double* row = Ws + (n - 16 - k) * n;
-      if (m0 < nt && m0 != k) h0 += row[n - 16 - m0];
-      if (m1 < nt && m1 != k) h1 += row[n - 16 - m1];
-      if (lane < 8) f += row[n - 1 - lane];
+    // Every lane keeps the t_hi state (fp64, lane-redundant): fh = t_hi^T W_ThU, gh =
+    // t_hi^T W_ThY, eh = E(t_hi), c_k = coupling of t_lo bit k with t_hi; lane l also
+    // keeps the fields of t_hi bits l and l + 32 from the other t_hi bits.
+    const int nh = nt - 5;  // t_hi bits: t bit 5 + m <-> variable n-21-m
+    double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) fh[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) gh[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) c[k] = 0.0;
+    const uint64_t th0 = t0 >> 5;
+    for (int m = 0; m < nh; ++m) {
+      if (!((th0 >> m) & 1)) continue;
+      const double* row = Ws + (n - 21 - m) * n;
+      eh += row[n - 21 - m];
+      for (int m2 = 0; m2 < m; ++m2)
+        if ((th0 >> m2) & 1) eh += row[n - 21 - m2];
+      if (lane < nh && lane != m) h0 += row[n - 21 - lane];
+      if (lane + 32 < nh && lane + 32 != m) h1 += row[n - 21 - lane - 32];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fh[k] += row[n - 1 - k];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) gh[k] += row[n - 9 - k];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) c[k] += row[n - 16 - k];
     }
-    for (uint64_t j = 0; j < ntiles && ok; ++j) {
+    for (uint64_t j0 = 0; j0 < ntiles && ok; j0 += 32) {
+      const uint64_t i0 = i_begin + j0;
+      if (j0 > 0) {  // t_hi changes by one bit between aligned runs of 32 Gray tiles
+        const int kb = __ffsll((long long)i0) - 1;  // >= 5
+        const int m = kb - 5;
+        const double sg = ((gray64(i0) >> kb) & 1) ? 1.0 : -1.0;
+        const double hm = __shfl_sync(0xffffffffu, m < 32 ? h0 : h1, m & 31);
+        const double* row = Ws + (n - 21 - m) * n;
+        eh += sg * (row[n - 21 - m] + hm);
+        if (lane < nh && lane != m) h0 += sg * row[n - 21 - lane];
+        if (lane + 32 < nh && lane + 32 != m) h1 += sg * row[n - 21 - lane - 32];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) fh[k] += sg * row[n - 1 - k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gh[k] += sg * row[n - 9 - k];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) c[k] += sg * row[n - 16 - k];
+      }
+      // this lane's tile
+      const uint64_t j = j0 + (uint64_t)lane;
+      const int tl = (int)(gray64(i0 + (uint64_t)lane) & 31ull);
+      const double* lo = LO + tl * 16;
+      double et = eh + lo[15];
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if ((tl >> k) & 1) et += c[k];
       const int s = (int)(j % kTcParamSlots);
-      const uint32_t ph = (uint32_t)((j / kTcParamSlots) & 1);
-      ok = mbar_wait(&p_empty[s], ph ^ 1u, abort_flag);
+      ok = mbar_wait(&p_empty[s], (uint32_t)(((j / kTcParamSlots) & 1) ^ 1), abort_flag);
+      ok = __all_sync(0xffffffffu, ok);  // keep the warp converged for the next shuffle
       if (!ok) break;
       TcSlot& sl = slots[s];
-      if (j == 0) {
-        if (lane == 0) {
-          sl.k = -1;
-          sl.sgn = 0.f;
-          sl.d = 0.0;
-        }
-      } else {
-        const uint64_t i = i_begin + j;
-        const int kb = __ffsll((long long)i) - 1;
-        const bool on = (gray64(i) >> kb) & 1;
-        const double sg = on ? 1.0 : -1.0;
-        const double hk = __shfl_sync(0xffffffffu, kb < 32 ? h0 : h1, kb & 31);
-        const double* row = Ws + (n - 16 - kb) * n;
-        if (lane == 0) {
-          sl.k = kb;
-          sl.sgn = (float)sg;
-          sl.d = row[n - 16 - kb] + hk;
-        }
-        if (m0 < nt && m0 != kb) h0 += sg * row[n - 16 - m0];
-        if (m1 < nt && m1 != kb) h1 += sg * row[n - 16 - m1];
-        if (lane < 8) f += sg * row[n - 1 - lane];
-      }
-      // C tables: F[l] (l < 16) = sum of f_j over bits j of l; F[16 + l] over bits j+4
-      double acc = 0.0;
-      const int base = lane < 16 ? 0 : 4;
-      for (int jb = 0; jb < 4; ++jb) {
-        double fj = __shfl_sync(0xffffffffu, f, base + jb);
-        if (((lane & 15) >> jb) & 1) acc += fj;
-      }
-      sl.F[lane] = (float)acc;
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&p_full[s]);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sl.f[k] = (float)(fh[k] + lo[k]);
+#pragma unroll
+      for (int k = 0; k < 7; ++k) sl.g[k] = (float)(gh[k] + lo[8 + k]);
+      sl.et = (float)et;
+      mbar_arrive(&p_full[s]);
     }
   } else if (warp == 1) {
     // ---------------------------------------------------------- MMA issue
@@ -419,13 +468,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       uint64_t issued = 0;
       for (uint64_t j = 0; j < ntiles && ok; ++j) {
         const int bs = (int)(j % kTcBStages);
-        const int as = (int)(j & 1);
+        const int as = (int)(j % kTcStages);
         ok = mbar_wait(&b_full[bs], (uint32_t)((j / kTcBStages) & 1), abort_flag) &&
-             mbar_wait(&acc_empty[as], (uint32_t)(((j >> 1) & 1) ^ 1), abort_flag);
+             mbar_wait(&acc_empty[as], (uint32_t)(((j / kTcStages) & 1) ^ 1), abort_flag);
         if (!ok) break;
         tc_fence_after();
-        const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * 256 * 32), 128, 256);
-        tc_mma(tmem + (uint32_t)as * 256u, adesc, bdesc);
+        const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
+        tc_mma(tmem + (uint32_t)as * (uint32_t)kTcN, adesc, bdesc);
         tc_commit(&b_empty[bs]);
         tc_commit(&acc_full[as]);
         issued = j + 1;
@@ -438,26 +487,34 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     __syncwarp();
   } else if (warp < 4) {
     // ---------------------------------------------------------- B producers (C_t columns)
-    const int pt = tid - 64;  // 0..63
-    for (uint64_t j = 0; j < ntiles && ok; ++j) {
+    // warp 2 + (j & 1) fills tile j: rows u = lane + 32 r, r < 8 (u bits 5..7 = r)
+    for (uint64_t j = (uint64_t)(warp - 2); j < ntiles && ok; j += 2) {
       const int s = (int)(j % kTcParamSlots);
       const int bs = (int)(j % kTcBStages);
       ok = mbar_wait(&p_full[s], (uint32_t)((j / kTcParamSlots) & 1), abort_flag);
-      float c[4];
-      if (ok) {
-        const TcSlot& sl = slots[s];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int u = pt + 64 * r;
-          c[r] = EU[u] + sl.F[u & 15] + sl.F[16 + (u >> 4)];
-        }
-        ok = mbar_wait(&b_empty[bs], (uint32_t)(((j / kTcBStages) & 1) ^ 1), abort_flag);
-      }
       if (!ok) break;
-      unsigned char* Bst = Bsm + bs * 256 * 32;
+      __half2 dg[8];
+      {
+        const TcSlot& sl = slots[s];
+        float s5 = 0.f;
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
-        *reinterpret_cast<__half2*>(Bst + kmaj_off(pt + 64 * r, 14)) = digits(c[r], P.exact);
+        for (int jb = 0; jb < 5; ++jb)
+          if ((lane >> jb) & 1) s5 += sl.f[jb];
+        const float f5 = sl.f[5], f6 = sl.f[6], f7 = sl.f[7];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          float cr = s5;
+          if (r & 1) cr += f5;
+          if (r & 2) cr += f6;
+          if (r & 4) cr += f7;
+          dg[r] = digits(EU[lane + 32 * r] + cr, P.exact);
+        }
+      }
+      ok = mbar_wait(&b_empty[bs], (uint32_t)(((j / kTcBStages) & 1) ^ 1), abort_flag);
+      if (!ok) break;
+      unsigned char* Bst = Bsm + bs * kTcN * 32;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
       fence_proxy_async();
       __syncwarp();
       if (lane == 0) {
@@ -467,63 +524,64 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     }
   } else {
     // ---------------------------------------------------------- epilogue
-    const int ew = warp - 4;  // 0..7
-    const int q = warp & 3;   // TMEM lane quarter (warp id % 4)
-    const int half = ew >> 2; // column half
+    const int q = warp & 3;           // TMEM lane quarter (warp id % 4)
+    const int cq = (warp - 4) >> 2;   // column quarter: columns 64*cq .. 64*cq+63
     const int y = q * 32 + lane;
-    double R = *ET0;
+    float ybit[7];
+#pragma unroll
+    for (int i = 0; i < 7; ++i) ybit[i] = (float)((y >> i) & 1);
+    float ey;  // E_Y(y)
     {
-      const double* yr = Ws + (n - 9) * n;  // placeholder row pointer (unused when y == 0)
-      (void)yr;
+      double e = 0.0;
       for (int i = 0; i < 7; ++i) {
         if (!((y >> i) & 1)) continue;
         const double* row = Ws + (n - 9 - i) * n;
-        R += row[n - 9 - i];
+        e += row[n - 9 - i];
         for (int i2 = 0; i2 < i; ++i2)
-          if ((y >> i2) & 1) R += row[n - 9 - i2];
+          if ((y >> i2) & 1) e += row[n - 9 - i2];
       }
-      for (int k = 0; k < nt; ++k)
-        if ((t0 >> k) & 1) R += hY[k * 128 + y];
+      ey = (float)e;
     }
     const float inv = P.inv_scale;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
     const uint64_t gmask = (1ull << P.gl) - 1ull;
-    const uint32_t lane_base = (uint32_t)(q * 32) << 16;
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)cq * 64u;
     for (uint64_t j = 0; j < ntiles && ok; ++j) {
       const int s = (int)(j % kTcParamSlots);
-      const int as = (int)(j & 1);
+      const int as = (int)(j % kTcStages);
       ok = mbar_wait(&p_full[s], (uint32_t)((j / kTcParamSlots) & 1), abort_flag);
       if (!ok) break;
+      float R;
       {
         const TcSlot& sl = slots[s];
-        if (sl.k >= 0) R += (double)sl.sgn * (sl.d + hY[sl.k * 128 + y]);
+        R = sl.et + ey;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) R = fmaf(ybit[i], sl.g[i], R);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&p_empty[s]);
-      ok = mbar_wait(&acc_full[as], (uint32_t)((j >> 1) & 1), abort_flag);
+      ok = mbar_wait(&acc_full[as], (uint32_t)((j / kTcStages) & 1), abort_flag);
       if (!ok) break;
       tc_fence_after();
-      const uint32_t ta = tmem + lane_base + (uint32_t)as * 256u + (uint32_t)half * 128u;
+      const uint32_t ta = tbase + (uint32_t)as * (uint32_t)kTcN;
       uint32_t ra[32], rb[32];
       QB_TC_LD32(ta, ra);
       QB_TC_LD32(ta + 32, rb);
       tc_wait_ld();
-      float m = fminf(min32(ra), min32(rb));
-      QB_TC_LD32(ta + 64, ra);
-      QB_TC_LD32(ta + 96, rb);
-      tc_wait_ld();
-      m = fmin3(m, min32(ra), min32(rb));
+      reg_fence32(ra);
+      reg_fence32(rb);
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[as]);
-      rmin = fminf(rmin, m + (float)R);
+      if (lane == 0) mbar_arrive(&acc_empty[as]);  // the stage is free once the data is in registers
+      const float m = fminf(min32(ra), min32(rb));
+      rmin = fminf(rmin, m + R);
       const uint64_t i = i_begin + j;
       if ((i & gmask) == gmask) {
         const float wm = warp_min_f(rmin);
         if (lane == 0) {
           const uint64_t J = (i >> P.gl) - (P.tile_begin >> P.gl);
-          P.rec[(J << 3) | ((uint64_t)half << 2) | (uint64_t)q] = wm * inv;
+          P.rec[(J << 4) | ((uint64_t)cq << 2) | (uint64_t)q] = wm * inv;
         }
         rmin = inf;
       }
