@@ -1,0 +1,328 @@
+"""Benchmark: states/s of the exhaustive search on the n=36 integer QUBO (6-city TSP with
+integer distances, seed 0), tensor-core form, with the plain Gray-code form and the CPU
+restatement of the reference timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form tc|gray]
+
+One step = one full exhaustive solve (pass 1 over all 2^36 states, candidate re-evaluation,
+tie rule) of the same problem.  For N > 1 (torchrun, one process per GPU) every rank searches
+its share of the tiles and the ranks exchange their minima (NCCL); the job is the same
+2^36 states ("scaling": "strong").  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOPS_PER_STATE_TC = 32  # one K=16 f16 MMA element per state: 16 multiply-adds
+N_VARS = 36
+WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), "measured"
+    return 1590.0, 1400.0, "fallback"
+
+
+def _traffic_per_state():
+    """DRAM bytes per state of the tensor-core kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "tc_pass1_kernel.traffic.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["dram_bytes_per_state"])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for ln in open(self.path):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) >= 9 and parts[1].isdigit():
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [int(r[1]) for r in rows]
+        mx = int(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [v for v in sm if v > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def _slice_solver(Q):
+    """Returns run(m): the CPU restatement of the reference (QBF's prefix loop under
+    Parallel's bit fixing, oracle/qbf_port.c) on all host cores over a slice of the
+    problem -- the first n - m variables fixed to 0 (one ReducedProblem task of the
+    reference's Parallel) and the remaining 2^m states searched -- timed in seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ctypes
+    import numpy as np
+    import oracle
+    cores = len(os.sched_getaffinity(0))
+    n = Q.shape[0]
+    Qf = np.ascontiguousarray(np.asarray(Q, dtype=np.float64))
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def run(m):
+        Qr = np.zeros((m, m))
+        oracle.lib().oq_reduce(n, Qf.ctypes.data_as(dp), n - m, 0, Qr.ctypes.data_as(dp))
+        splits = 1 << max(0, min(m - 20, (cores - 1).bit_length() + 2))
+        t = time.perf_counter()
+        oracle.parallel_port(np.rint(Qr).astype(np.int64), splits, nthreads=cores)
+        return time.perf_counter() - t, splits
+
+    return run, cores
+
+
+def _calibrate(run, n, budget_s):
+    m = 28
+    dt, splits = run(m)
+    while dt < budget_s / 4 and m < n - 1:
+        m += 2 if dt < budget_s / 16 else 1
+        dt, splits = run(m)
+    return m, dt, splits
+
+
+def _sample_text(m, n, splits, dt):
+    return (f"2^{m} states: the first {n - m} variables fixed to 0, Parallel bit fixing into {splits} "
+            f"QBF tasks (B = 20 prefix loop), {dt:.1f} s")
+
+
+def cpu_baseline(Q, budget_s: float = 15.0) -> dict:
+    run, cores = _slice_solver(Q)
+    n = Q.shape[0]
+    m, dt, splits = _calibrate(run, n, budget_s)
+    return {"value": (1 << m) / dt, "unit": "states/s", "cores": cores, "kind": "port",
+            "sample": _sample_text(m, n, splits, dt)}
+
+
+def bench_reference(args):
+    """The reference arm: the CPU restatement of the reference's algorithm (the reference is
+    a Python/cupy package that is not installed on the GPU host) on all host cores; each
+    step searches one bounded slice of the same 36-variable problem."""
+    from qubo_b200 import configs
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    Q = configs.tsp6_int()
+    n = Q.shape[0]
+    run, cores = _slice_solver(Q)
+    m, dt, splits = _calibrate(run, n, 12.0)  # also the warm-up
+    for _ in range(max(0, args.warmup - 1)):
+        run(m)
+    times = [run(m)[0] for _ in range(args.steps)]
+    value = (1 << m) * len(times) / sum(times)
+    sample = _sample_text(m, n, splits, sum(times) / len(times))
+    line = {"metric": "states/s (exhaustive QUBO, exact argmin)", "value": value, "unit": "states/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "sample": sample},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "states/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "states/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def bench_ours(args):
+    import numpy as np
+    import torch
+    import qubo_b200  # noqa: F401
+    from qubo_b200 import _lib, configs
+    from qubo_b200.problems import Just_Q
+    from qubo_b200.solvers import QBF
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    Q = configs.tsp6_int()
+    n = Q.shape[0]
+    states = 1 << n
+    Qd = torch.as_tensor(Q, device=f"cuda:{local}")  # inputs resident in HBM
+    stream = torch.cuda.current_stream(local)
+    h = _lib.handle(local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
+
+    def step(form):
+        if world == 1:
+            return h.solve_device(Qd.data_ptr(), n, Q.dtype, form=form, tie_rule="qbf", prefix_bits=-1,
+                                  stream=stream.cuda_stream)
+        from qubo_b200.distributed import solve_sharded
+        return solve_sharded(Q, form=form, device=local, Q_device_ptr=Qd.data_ptr())
+
+    def timed(form, steps, warmup):
+        for _ in range(warmup):
+            step(form)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        res = []
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            res.append(step(form))
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        if dist is not None:
+            dist.barrier()
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item()) / steps, res
+
+    form = args.form
+    with ClockSampler(local) as clk:
+        ms, res = timed(form, args.steps, args.warmup)
+    clocks = clk.summary()
+    gray_ms, gres = timed("gray", max(3, args.steps // 2), 3)
+    r0 = res[-1]
+    # e2e: the public API with a host-resident problem, H2D and D2H inside the timed region
+    prob = Just_Q(Q)
+    e2e_times, h2d, d2h = [], 0, 0
+    for k in range(args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if world == 1:
+            sol = QBF().solve(prob, device=f"cuda:{local}", form=form)
+            rr = sol.search
+            h2d_k, d2h_k = rr.get("h2d_bytes", 0), rr.get("d2h_bytes", 0)
+        else:
+            from qubo_b200.distributed import solve_sharded
+            rr = solve_sharded(Q, form=form, device=local)
+            h2d_k, d2h_k = rr["h2d_bytes"], rr["d2h_bytes"]
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_times.append(t1 - t0)
+            h2d, d2h = h2d_k, d2h_k
+    e2e_s = torch.tensor([sum(e2e_times) / len(e2e_times)], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+    e2e_value = states / float(e2e_s.item())
+
+    kernel_ms = statistics.mean(r["kernel_ms"] for r in res)
+    peak, peak_sus, peak_kind = _peaks()
+    local_states = r0["states"] if world == 1 else r0["states"]
+    achieved = local_states * FLOPS_PER_STATE_TC / (kernel_ms * 1e-3) / 1e12
+    tps = _traffic_per_state()
+    line = {
+        "metric": "states/s (exhaustive QUBO, exact argmin)",
+        "value": states / (ms * 1e-3),
+        "unit": "states/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "strong",
+        "vs_baseline": None,
+        "dtype": "f32 (f16 digit operands, fp32 accumulate; exact for this integer Q)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "form": form, "states_per_step": states,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"tile shards x{world}",
+                   "answer": {"best_E": r0["best_E"], "best_X": int(r0["best_X_int"])}},
+        "e2e": {"value": e2e_value, "unit": "states/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(sum(r["kernels"] for r in res)),
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": (tps * local_states if tps is not None else None),
+                     "peak_kind": f"bf16 dense burst, {peak_kind}", "kernel_ms": kernel_ms,
+                     "flops_per_state": FLOPS_PER_STATE_TC},
+        "gray_form": {"value": states / (gray_ms * 1e-3), "ms_per_step": gray_ms,
+                      "kernel_ms": statistics.mean(r["kernel_ms"] for r in gres)},
+        "tc_over_gray": (gray_ms / ms),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1:
+        line["cpu_baseline"] = cpu_baseline(Q)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_case(args):
+    """A small profiling case: the 32-variable integer QUBO (RandomQUBO seed 0, entries in
+    [-100, 100], symmetric int16), solved `steps` times with one form; prints one line per
+    solve.  Used for ncu captures of a single kernel (a few MB on the device)."""
+    import torch
+    import qubo_b200  # noqa: F401
+    from qubo_b200 import _lib, configs
+    torch.cuda.set_device(0)
+    Q = configs.random_i16_n32()
+    h = _lib.handle(0)
+    stream = torch.cuda.current_stream(0).cuda_stream
+    for k in range(args.warmup + args.steps):
+        r = h.solve(Q, form=args.form, stream=stream)
+        if k >= args.warmup:
+            print(json.dumps({"case": "random_i16_n32", "form": r["form"], "best_E": r["best_E"],
+                              "kernel_ms": r["kernel_ms"], "pass1_ms": r["pass1_ms"], "pass2_ms": r["pass2_ms"]}),
+                  flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto"])
+    ap.add_argument("--case", default=None, choices=["cfg2"], help="small profiling case instead of the benchmark")
+    args = ap.parse_args()
+    if args.case:
+        bench_case(args)
+    elif args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -47,7 +47,7 @@ class QbResult(ctypes.Structure):
                 ("states", ctypes.c_int64), ("candidate_records", ctypes.c_int64), ("form_used", ctypes.c_int32),
                 ("is_integer", ctypes.c_int32), ("found", ctypes.c_int32), ("status", ctypes.c_int32),
                 ("pass1_ms", ctypes.c_float), ("pass2_ms", ctypes.c_float), ("kernels", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("kernel_ms", ctypes.c_float), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
 
 
 class QbError(RuntimeError):
@@ -150,6 +150,25 @@ class Handle:
             _raise(rc, "qb_solve")
         return result_dict(r, p.n)
 
+    def solve_device(self, ptr: int, n: int, dtype, **opts) -> dict:
+        """Solve a Q already resident in device memory (row-major n x n at `ptr`)."""
+        p = QbProblem(n=int(n), dtype=_DTYPES[np.dtype(dtype)], q=int(ptr), ldq=int(n), q_on_device=1)
+        o = self.options(**opts)
+        r = QbResult()
+        rc = load().qb_solve(self._h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(r))
+        if rc:
+            _raise(rc, "qb_solve")
+        return result_dict(r, int(n))
+
+    def solve_begin_device(self, ptr: int, n: int, dtype, **opts) -> float:
+        p = QbProblem(n=int(n), dtype=_DTYPES[np.dtype(dtype)], q=int(ptr), ldq=int(n), q_on_device=1)
+        o = self.options(**opts)
+        v = ctypes.c_double()
+        rc = load().qb_solve_begin(self._h, ctypes.byref(p), ctypes.byref(o), ctypes.byref(v))
+        if rc:
+            _raise(rc, "qb_solve_begin")
+        return v.value
+
     def solve_begin(self, Q: np.ndarray, **opts) -> float:
         p, keep = self._problem(Q)
         o = self.options(**opts)
@@ -207,6 +226,9 @@ def result_dict(r: QbResult, n: int) -> dict:
         "pass1_ms": float(r.pass1_ms),
         "pass2_ms": float(r.pass2_ms),
         "kernels": int(r.kernels),
+        "kernel_ms": float(r.kernel_ms),
+        "h2d_bytes": int(r.h2d_bytes),
+        "d2h_bytes": int(r.d2h_bytes),
     }
 
 

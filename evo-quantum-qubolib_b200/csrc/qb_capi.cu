@@ -95,7 +95,9 @@ struct qb_handle_s {
   cudaStream_t st = nullptr;
   DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
   HostBuf hW, hmisc, hout;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // 4, 5: main kernel
+  int64_t h2d = 0, d2h = 0;  // bytes copied by the current call
+  float kernel_ms = 0.f;
   int sm_count = 0;
   // state between qb_solve_begin and qb_solve_finish
   bool pending = false;
@@ -153,6 +155,7 @@ int load_problem(qb_handle* h, const qb_problem* p, std::vector<double>& W, doub
     QB_CUDA(cudaMemcpy2DAsync(raw.data(), (size_t)n * es, p->q, (size_t)p->ldq * es, (size_t)n * es, n,
                               cudaMemcpyDeviceToHost, h->st));
     QB_CUDA(cudaStreamSynchronize(h->st));
+    h->d2h += (int64_t)n * n * es;
   } else {
     const unsigned char* src = static_cast<const unsigned char*>(p->q);
     for (int i = 0; i < n; ++i) memcpy(raw.data() + (size_t)i * n * es, src + (size_t)i * p->ldq * es, (size_t)n * es);
@@ -281,6 +284,7 @@ int upload_W(qb_handle* h, const std::vector<double>& W) {
   QB_CUDA(h->W.ensure(bytes));
   memcpy(h->hW.p, W.data(), bytes);
   QB_CUDA(cudaMemcpyAsync(h->W.p, h->hW.p, bytes, cudaMemcpyHostToDevice, h->st));
+  h->h2d += (int64_t)bytes;
   return QB_OK;
 }
 
@@ -292,6 +296,7 @@ int run_pass1(qb_handle* h, Plan& P) {
     QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     // chunked over the grid limit
     const uint64_t maxg = 1u << 30;
+    QB_CUDA(cudaEventRecord(h->ev[4], h->st));
     for (uint64_t off = 0; off < P.rec_count; off += maxg) {
       uint64_t g = std::min<uint64_t>(maxg, P.rec_count - off);
       qb::exact_records_kernel<<<(unsigned)g, qb::kExactThreads, sm, h->st>>>(
@@ -299,6 +304,7 @@ int run_pass1(qb_handle* h, Plan& P) {
           static_cast<qb::ExactOut*>(h->exout.p) + off);
       ++h->kernels;
     }
+    QB_CUDA(cudaEventRecord(h->ev[5], h->st));
     QB_CUDA(cudaGetLastError());
     return QB_OK;
   }
@@ -323,16 +329,23 @@ int run_pass1(qb_handle* h, Plan& P) {
     size_t sm = qb::gray_pass1_smem(P.n, P.a);
     QB_CUDA(cudaFuncSetAttribute(qb::gray_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     uint64_t units = P.unit_end - P.unit_begin;
+    QB_CUDA(cudaEventRecord(h->ev[4], h->st));
     if (units) {
       qb::gray_pass1_kernel<<<(unsigned)units, qb::kGrayThreads, sm, h->st>>>(gp);
       ++h->kernels;
     }
+    QB_CUDA(cudaEventRecord(h->ev[5], h->st));
     QB_CUDA(cudaGetLastError());
     return QB_OK;
   }
   QB_CUDA(h->tcscratch.ensure(qb::tc_scratch_bytes(P.tc)));
-  int rc = qb::tc_launch(P.tc, pd, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st, h->sm_count, &h->kernels);
-  return rc;
+  int rc = qb::tc_prepare(P.tc, pd, h->tcscratch.p, h->st, &h->kernels);
+  if (rc) return rc;
+  QB_CUDA(cudaEventRecord(h->ev[4], h->st));
+  rc = qb::tc_launch(P.tc, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st, h->sm_count, &h->kernels);
+  if (rc) return rc;
+  QB_CUDA(cudaEventRecord(h->ev[5], h->st));
+  return QB_OK;
 }
 
 }  // namespace
@@ -368,7 +381,7 @@ int qb_handle_create(int device, qb_handle** out) {
   qb_handle* h = new qb_handle_s();
   h->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking);
-  for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+  for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) {
     qb_handle_destroy(h);
@@ -408,6 +421,7 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
   h->st = o->stream ? static_cast<cudaStream_t>(o->stream) : h->own;
   h->pending = false;
   h->kernels = 0;
+  h->h2d = h->d2h = 0;
   h->cap = o->max_candidates > 0 ? o->max_candidates : kDefaultCap;
   Plan P;
   P.n = p->n;
@@ -432,6 +446,7 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
     size_t bytes = P.rec_count * sizeof(qb::ExactOut);
     QB_CUDA(h->hout.ensure(std::max<size_t>(bytes, 64)));
     if (bytes) QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, bytes, cudaMemcpyDeviceToHost, h->st));
+    h->d2h += (int64_t)bytes;
     QB_CUDA(cudaStreamSynchronize(h->st));
     const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
     for (uint64_t i = 0; i < P.rec_count; ++i) lmin = std::min(lmin, eo[i].e);
@@ -447,15 +462,18 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
     }
     QB_CUDA(cudaEventRecord(h->ev[1], h->st));
     QB_CUDA(cudaMemcpyAsync(h->hmisc.p, mk, sizeof(uint32_t), cudaMemcpyDeviceToHost, h->st));
+    h->d2h += (int64_t)sizeof(uint32_t);
     QB_CUDA(cudaStreamSynchronize(h->st));
     if (P.form == QB_FORM_TC) {
       int trc = qb::tc_check_error(h->tcscratch.p, h->st);
+      h->d2h += (int64_t)sizeof(unsigned);
       if (trc) return trc;
     }
     uint32_t key = *static_cast<uint32_t*>(h->hmisc.p);
     lmin = (P.rec_count && key != 0xffffffffu) ? (double)qb::key2f(key) : INFINITY;
   }
   QB_CUDA(cudaEventElapsedTime(&h->pass1_ms, h->ev[0], h->ev[1]));
+  QB_CUDA(cudaEventElapsedTime(&h->kernel_ms, h->ev[4], h->ev[5]));
   h->plan = P;
   h->local_min = lmin;
   h->pending = true;
@@ -488,6 +506,7 @@ int rescore(qb_handle* h, const Plan& P, const qb::TieRule& rule, const qb::RecG
   QB_CUDA(cudaGetLastError());
   QB_CUDA(h->hout.ensure((size_t)count * sizeof(qb::ExactOut)));
   QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, (size_t)count * sizeof(qb::ExactOut), cudaMemcpyDeviceToHost, h->st));
+  h->d2h += (int64_t)count * (int64_t)sizeof(qb::ExactOut);
   QB_CUDA(cudaStreamSynchronize(h->st));
   const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
   out.assign(eo, eo + count);
@@ -508,6 +527,7 @@ int qbf1_row(qb_handle* h, const Plan& P, uint64_t X, double e_star, uint64_t* X
   uint64_t rid = X >> 18;
   QB_CUDA(h->cand.ensure(sizeof(uint64_t)));
   QB_CUDA(cudaMemcpyAsync(h->cand.p, &rid, sizeof(uint64_t), cudaMemcpyHostToDevice, h->st));
+  h->h2d += (int64_t)sizeof(uint64_t);
   std::vector<qb::ExactOut> o;
   int rc = rescore(h, P, nat, g, 1, o);
   if (rc) return rc;
@@ -561,6 +581,7 @@ int qb_solve_finish(qb_handle* h, double global_min, qb_result* r) {
         QB_CUDA(cudaGetLastError());
       }
       QB_CUDA(cudaMemcpyAsync(h->hmisc.p, cnt, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+      h->d2h += (int64_t)sizeof(int);
       QB_CUDA(cudaStreamSynchronize(h->st));
       count = *static_cast<int*>(h->hmisc.p);
       if (count <= h->cap) break;
@@ -593,6 +614,9 @@ int qb_solve_finish(qb_handle* h, double global_min, qb_result* r) {
   r->best_e_int = (found && P.is_int) ? (int64_t)llround(best.e) : 0;
   r->order_key = best.key;
   r->kernels = h->kernels;
+  r->kernel_ms = h->kernel_ms;
+  r->h2d_bytes = h->h2d;
+  r->d2h_bytes = h->d2h;
   r->status = QB_OK;
   return QB_OK;
 }

@@ -604,15 +604,22 @@ __global__ void tc_scale_w_kernel(const double* __restrict__ W, double* __restri
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) out[i] = W[i] * scale;
 }
 
-inline int tc_launch(const TcPlan& p, ProblemDev pd, float* rec, void* scratch, cudaStream_t st, int sms,
-                     int* kernels) {
+// clears the error word and writes the scaled W into the scratch buffer
+inline int tc_prepare(const TcPlan& p, ProblemDev pd, void* scratch, cudaStream_t st, int* kernels) {
   unsigned* err = static_cast<unsigned*>(scratch);
   double* Wsc = reinterpret_cast<double*>(static_cast<char*>(scratch) + 16);
   if (cudaMemsetAsync(err, 0, 16, st) != cudaSuccess) return 4;
   tc_scale_w_kernel<<<8, 256, 0, st>>>(pd.W, Wsc, p.n * p.n, p.scale);
   ++*kernels;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+
+// the search kernel itself (one persistent CTA per SM)
+inline int tc_launch(const TcPlan& p, float* rec, void* scratch, cudaStream_t st, int sms, int* kernels) {
+  unsigned* err = static_cast<unsigned*>(scratch);
+  double* Wsc = reinterpret_cast<double*>(static_cast<char*>(scratch) + 16);
   const uint64_t groups = (p.tile_end - p.tile_begin) >> p.gl;
-  if (!groups) return cudaGetLastError() == cudaSuccess ? 0 : 4;
+  if (!groups) return 0;
   uint64_t ctas = std::min<uint64_t>((uint64_t)sms, groups);
   uint64_t gpc = (groups + ctas - 1) / ctas;
   ctas = (groups + gpc - 1) / gpc;

@@ -159,7 +159,8 @@ class QBF(SolverABC):
         sol.time_to_solve_ms = self.timer.get_time_from_start()
         sol.timer = [(t, lbl) for t, lbl in self.timer.times if lbl != "epoch"]
         sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_min", "err_bound",
-                                          "pass1_ms", "pass2_ms", "order_key", "kernels")}
+                                          "pass1_ms", "pass2_ms", "kernel_ms", "order_key", "kernels",
+                                          "h2d_bytes", "d2h_bytes")}
         sol.search["split"] = (self.A, self.B)
         return sol
 
@@ -213,7 +214,8 @@ class QB_F1(SolverABC):
         sol.ising_offset = problem.get_Q_Ising_offset(np, Q)
         sol.timer = [(t, lbl) for t, lbl in self.timer.times if lbl != "epoch"]
         sol.time_to_solve_ms = self.timer.get_time_from_start()
-        sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_ms", "pass2_ms", "kernels")}
+        sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_ms", "pass2_ms", "kernel_ms",
+                                          "kernels", "h2d_bytes", "d2h_bytes")}
         sol.search["int16_wrap_possible"] = _int16_wrap_possible(Q)
         if sol.search["int16_wrap_possible"]:
             logger.warning("QB_F1: partial sums of Q exceed int16; the reference's int16 arithmetic could wrap, "

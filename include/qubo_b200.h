@@ -103,7 +103,9 @@ typedef struct qb_result {
   float pass1_ms;         /* device time of pass 1 (CUDA events) */
   float pass2_ms;         /* device time of reduction + candidate re-evaluation */
   int32_t kernels;        /* kernel launches issued by this call */
-  int32_t reserved;
+  float kernel_ms;        /* device time of the main pass-1 search kernel alone */
+  int64_t h2d_bytes;      /* bytes copied host -> device by this call */
+  int64_t d2h_bytes;      /* bytes copied device -> host by this call */
 } qb_result;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
