@@ -14,7 +14,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libqubo_b200.so")
 
-QB_OK, QB_EINVAL, QB_ERANGE, QB_ENOMEM, QB_ECUDA, QB_ETIMEOUT, QB_ENODEV, QB_EOVERFLOW = range(8)
+QB_OK, QB_EINVAL, QB_ERANGE, QB_ENOMEM, QB_ECUDA, QB_ETIMEOUT, QB_ENODEV, QB_EOVERFLOW, QB_ETOOBIG = range(9)
 QB_F32, QB_F64, QB_I8, QB_I16, QB_I32, QB_I64 = 1, 2, 3, 4, 5, 6
 FORMS = {"auto": 0, "gray": 1, "tc": 2, "exact": 3}
 FORM_NAMES = {v: k for k, v in FORMS.items()}
@@ -50,6 +50,11 @@ class QbResult(ctypes.Structure):
                 ("kernel_ms", ctypes.c_float), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
 
 
+class QbNoAllocResult(ctypes.Structure):
+    _fields_ = [("best_e", ctypes.c_double), ("best_x", ctypes.c_uint64), ("order_key", ctypes.c_uint64),
+                ("status", ctypes.c_int32), ("candidates", ctypes.c_int32)]
+
+
 class QbError(RuntimeError):
     def __init__(self, status: int, where: str):
         self.status = status
@@ -82,6 +87,8 @@ def load():
     L.qb_solve_batch.argtypes = [H, ctypes.POINTER(QbProblem), ctypes.c_int32, ctypes.POINTER(QbOptions),
                                  ctypes.POINTER(QbResult)]
     L.qb_autotune.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.qb_solve_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                   ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
     return L
 

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace {
@@ -364,6 +365,7 @@ const char* qb_strerror(int s) {
     case QB_ETIMEOUT: return "a bounded wait inside a kernel timed out";
     case QB_ENODEV: return "no such CUDA device";
     case QB_EOVERFLOW: return "too many candidate records";
+    case QB_ETOOBIG: return "problem larger than the fixed no-allocation scratch (qb_solve_noalloc: 20 <= n <= 36)";
     default: return "unknown status";
   }
 }
@@ -651,3 +653,230 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// qb_solve_noalloc: the whole Gray-form search on the caller's stream with no allocation.
+//
+// Some callers cannot allocate device memory during a solve: an application that hands
+// out all of its device memory from its own pool up front, a real-time loop that must not
+// block on the allocator (cudaMalloc and cudaFree synchronise the device), or code running
+// where a new allocation would break a memory budget fixed at start-up.  For them this
+// entry point keeps every intermediate buffer in one file-scope device array of fixed size
+// (kNoAllocBytes, 16.9 MB) that each GPU holds from the moment the library's device code is
+// loaded on it until the process exits.  The caller passes Q and the output on the device; the entry
+// point calls no cudaMalloc, cudaFree, cudaMallocHost or allocating library routine and
+// does not wait for the GPU.
+//
+// Set-up: the first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that first call
+// before any stream capture.  All calls share the one array and every call overwrites it:
+// calls whose work overlaps on the GPU (other streams, other threads) race and must be
+// serialised by the caller.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxN = 36;
+constexpr int kNoAllocMinN = 20;
+constexpr int kNoAllocCands = 4096;
+constexpr size_t kNoAllocW = 16 * 1024;                             // n*n doubles, n <= 36
+constexpr size_t kNoAllocGtab = (size_t)1 << 16 << 5 << 2;          // 2^16 prefix steps x 32 floats
+constexpr size_t kNoAllocRec = (size_t)1 << 21 << 2;                // 2^(n-10-sbits) <= 2^21 records x float
+constexpr size_t kNoAllocCand = (size_t)kNoAllocCands * sizeof(uint64_t);
+constexpr size_t kNoAllocOut = (size_t)kNoAllocCands * sizeof(qb::ExactOut);
+constexpr size_t kNoAllocMisc = 256;
+constexpr size_t kNoAllocBytes = kNoAllocW + kNoAllocGtab + kNoAllocRec + kNoAllocCand + kNoAllocOut + kNoAllocMisc;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocMisc {  // lives at the end of g_noalloc_scratch
+  double abs_sum;
+  double threshold;
+  uint32_t min_key;
+  int cand_count;
+};
+
+static_assert(sizeof(NoAllocMisc) <= kNoAllocMisc, "misc block");
+static_assert(kNoAllocBytes == 16924928, "scratch size stated in include/qubo_b200.h");
+
+std::mutex g_noalloc_lock;
+void* g_noalloc_addr[128] = {nullptr};
+
+__global__ void noalloc_prep_kernel(const double* __restrict__ Q, int n, double* __restrict__ W,
+                                    NoAllocMisc* __restrict__ misc) {
+  __shared__ double part[256];
+  double s = 0.0;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int i = e / n, j = e % n;
+    const double q = Q[e];
+    s += fabs(q);
+    W[e] = (i == j) ? q : q + Q[j * n + i];
+  }
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off; off >>= 1) {
+    if (threadIdx.x < off) part[threadIdx.x] += part[threadIdx.x + off];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    misc->abs_sum = part[0];
+    misc->min_key = 0xffffffffu;
+    misc->cand_count = 0;
+  }
+}
+
+__global__ void noalloc_threshold_kernel(NoAllocMisc* __restrict__ misc, int is_int) {
+  const double m = (double)qb::key2f(misc->min_key);
+  const double S = misc->abs_sum;
+  // the Gray form's per-state bound on |fp32 pass-1 value - exact energy| (300 ulp of S)
+  const double eps = (is_int && S < 16777216.0) ? 0.0 : 300.0 * S * 5.9604644775390625e-08;
+  double thr = m + 2.0 * eps;
+  if (eps > 0.0) thr += fabs(thr) * 1e-12;
+  misc->threshold = thr;
+  misc->cand_count = 0;
+}
+
+__global__ void noalloc_select_kernel(const float* __restrict__ rec, int64_t count, const NoAllocMisc* misc,
+                                      uint64_t* __restrict__ cand, int* __restrict__ cand_count, int cap) {
+  const double thr = misc->threshold;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+    if ((double)rec[i] <= thr) {
+      const int s = atomicAdd(cand_count, 1);
+      if (s < cap) cand[s] = (uint64_t)i;
+    }
+  }
+}
+
+__global__ void noalloc_final_kernel(const qb::ExactOut* __restrict__ eo, const NoAllocMisc* __restrict__ misc,
+                                     int cap, int is_int, qb_noalloc_result* __restrict__ out) {
+  __shared__ qb::ExactOut best[256];
+  const int cnt = misc->cand_count;
+  const int m = cnt < cap ? cnt : cap;
+  qb::ExactOut b{__longlong_as_double(0x7ff0000000000000ll), ~0ull, 0ull};
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    if (eo[i].e < b.e || (eo[i].e == b.e && eo[i].key < b.key)) b = eo[i];
+  best[threadIdx.x] = b;
+  __syncthreads();
+  for (int off = blockDim.x / 2; off; off >>= 1) {
+    if (threadIdx.x < off) {
+      const qb::ExactOut& o = best[threadIdx.x + off];
+      if (o.e < best[threadIdx.x].e || (o.e == best[threadIdx.x].e && o.key < best[threadIdx.x].key))
+        best[threadIdx.x] = o;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double pmin = (double)qb::key2f(misc->min_key);
+    const bool exact_int = is_int && misc->abs_sum < 16777216.0;
+    if (is_int && misc->abs_sum >= 9007199254740992.0) {  // sum |Q_ij| >= 2^53: FP64 not exact
+      out->best_e = 0.0;
+      out->best_x = 0ull;
+      out->order_key = 0ull;
+      out->status = QB_ERANGE;
+    } else if (exact_int && pmin >= 0.0) {  // E(0) = 0 is minimal; X = 0 has the smallest key
+      out->best_e = 0.0;
+      out->best_x = 0ull;
+      out->order_key = 0ull;
+      out->status = QB_OK;
+    } else {
+      out->best_e = best[0].e;
+      out->best_x = best[0].x;
+      out->order_key = best[0].key;
+      out->status = cnt > cap ? QB_EOVERFLOW : (m > 0 ? QB_OK : QB_ECUDA);
+    }
+    out->candidates = cnt;
+  }
+}
+
+// Queues the search on `st`; `device` is current.
+int noalloc_run(int device, const double* q_dev, int n, int is_integer, int prefix_bits, qb_noalloc_result* out_dev,
+                cudaStream_t st) {
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_lock);
+    if (!g_noalloc_addr[device]) {  // first call on this device: resolve the array's address
+      void* a = nullptr;
+      QB_CUDA(cudaGetSymbolAddress(&a, g_noalloc_scratch));
+      g_noalloc_addr[device] = a;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_addr[device]);
+  }
+  const int A = prefix_bits < 0 ? n - std::min(n, 20) : prefix_bits;
+  if (A > n) return QB_EINVAL;
+  double* W = reinterpret_cast<double*>(base);
+  float* gtab = reinterpret_cast<float*>(base + kNoAllocW);
+  float* rec = reinterpret_cast<float*>(base + kNoAllocW + kNoAllocGtab);
+  uint64_t* cand = reinterpret_cast<uint64_t*>(base + kNoAllocW + kNoAllocGtab + kNoAllocRec);
+  qb::ExactOut* eo = reinterpret_cast<qb::ExactOut*>(base + kNoAllocW + kNoAllocGtab + kNoAllocRec + kNoAllocCand);
+  NoAllocMisc* misc =
+      reinterpret_cast<NoAllocMisc*>(base + kNoAllocW + kNoAllocGtab + kNoAllocRec + kNoAllocCand + kNoAllocOut);
+  // the Gray-form plan of qb_solve for this n (one shard)
+  const int b = std::max(13, n - 16), a = n - b, cbbits = b - 13;
+  const int sbits = std::min(a, std::max(5, n - 34));
+  const int ubits = std::min(a, std::max(7, std::max(sbits, std::min(a, a + cbbits - 11))));
+  qb::RecGeom geom{};
+  geom.kind = qb::kGeomGray;
+  geom.n = n;
+  geom.a = a;
+  geom.b = b;
+  geom.sbits = sbits;
+  geom.cbbits = cbbits;
+  geom.gubits = ubits - sbits;
+  const uint64_t units = 1ull << (a - ubits + cbbits);
+  const uint64_t nrec = units << (geom.gubits + 3);
+  const qb::TieRule rule{qb::kTieQBF, n, 0, A, n - A};
+  int sms = 0;
+  QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const qb::ProblemDev pd{n, W};
+  noalloc_prep_kernel<<<1, 256, 0, st>>>(q_dev, n, W, misc);
+  const size_t sm0 = qb::gray_gtab_smem(n, a);
+  QB_CUDA(cudaFuncSetAttribute(qb::gray_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm0));
+  qb::gray_gtab_kernel<<<(unsigned)std::min<uint64_t>((1ull << a) / 8 + 1, (uint64_t)sms * 4), 256, sm0, st>>>(pd, a, b, gtab);
+  qb::GrayParams gp{};
+  gp.P = pd;
+  gp.a = a;
+  gp.b = b;
+  gp.cbbits = cbbits;
+  gp.sbits = sbits;
+  gp.gubits = geom.gubits;
+  gp.unit_begin = 0;
+  gp.gtab = gtab;
+  gp.rec = rec;
+  const size_t sm1 = qb::gray_pass1_smem(n, a);
+  QB_CUDA(cudaFuncSetAttribute(qb::gray_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  qb::gray_pass1_kernel<<<(unsigned)units, qb::kGrayThreads, sm1, st>>>(gp);
+  const unsigned rb = (unsigned)std::min<uint64_t>((nrec + 255) / 256, (uint64_t)sms * 8);
+  qb::rec_min_kernel<<<rb, 256, 0, st>>>(rec, (int64_t)nrec, &misc->min_key);
+  noalloc_threshold_kernel<<<1, 1, 0, st>>>(misc, is_integer ? 1 : 0);
+  noalloc_select_kernel<<<rb, 256, 0, st>>>(rec, (int64_t)nrec, misc, cand, &misc->cand_count, kNoAllocCands);
+  int maxf = 0;
+  {
+    uint64_t bb, ff;
+    qb::record_states(geom, 0, &bb, &ff);
+    maxf = __builtin_popcountll(ff & qb::mask64(n));
+  }
+  const size_t sm2 = qb::exact_smem_bytes(n, maxf);
+  QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  qb::exact_records_kernel<<<kNoAllocCands, qb::kExactThreads, sm2, st>>>(pd, rule, geom, cand, &misc->cand_count, 0, 0,
+                                                                         eo);
+  noalloc_final_kernel<<<1, 256, 0, st>>>(eo, misc, kNoAllocCands, is_integer ? 1 : 0, out_dev);
+  QB_CUDA(cudaGetLastError());
+  return QB_OK;
+}
+
+}  // namespace
+
+extern "C" int qb_solve_noalloc(int device, const double* q_dev, int32_t n, int32_t is_integer, int32_t prefix_bits,
+                                qb_noalloc_result* out_dev, void* stream) {
+  if (!q_dev || !out_dev) return QB_EINVAL;
+  if (n < kNoAllocMinN || n > kNoAllocMaxN) return QB_ETOOBIG;
+  int ndev = 0;
+  QB_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev || device >= 128) return QB_ENODEV;
+  int prev = 0;
+  QB_CUDA(cudaGetDevice(&prev));
+  if (prev != device) QB_CUDA(cudaSetDevice(device));
+  const int rc = noalloc_run(device, q_dev, n, is_integer, prefix_bits, out_dev, static_cast<cudaStream_t>(stream));
+  if (prev != device) cudaSetDevice(prev);
+  return rc;
+}

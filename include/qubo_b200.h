@@ -44,6 +44,7 @@ extern "C" {
 #define QB_ETIMEOUT 5    /* a bounded wait inside a kernel gave up */
 #define QB_ENODEV 6      /* no CUDA device / bad device index */
 #define QB_EOVERFLOW 7   /* too many candidate records (raise QB_MAX_CANDIDATES) */
+#define QB_ETOOBIG 8     /* qb_solve_noalloc: n outside the fixed scratch (20 <= n <= 36) */
 
 /* element types of Q */
 #define QB_F32 1
@@ -148,6 +149,36 @@ int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, cons
  * QB_FORM_AUTO.  *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond
  * QBF.define_chunk_size (src/qubo_lib/solvers/qbf.py:429-466), which picks a split. */
 int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out);
+
+/* Result written by qb_solve_noalloc into device memory. */
+typedef struct qb_noalloc_result {
+  double best_e;        /* E(best_x) in FP64 (exact for integer Q) */
+  uint64_t best_x;      /* MSB-first state integer */
+  uint64_t order_key;   /* QB_TIE_QBF key of best_x */
+  int32_t status;       /* QB_OK, or QB_EOVERFLOW when more candidate records than fit */
+  int32_t candidates;   /* candidate records found by the selection */
+} qb_noalloc_result;
+
+/* Exhaustive minimum and argmin (QB_TIE_QBF with prefix_bits, -1 = QBF default) of one
+ * problem, for callers that cannot allocate: an application that hands out all of its
+ * device memory from its own pool up front, a real-time loop that must not stall on the
+ * allocator (cudaMalloc / cudaFree synchronise the device), or code with a device-memory
+ * budget fixed at start-up.  No counterpart in the reference, whose solvers allocate
+ * (numpy / cupy) on every call.
+ *
+ * q_dev: n x n float64 Q on `device` (row-major); is_integer: Q holds integers (exact
+ * search); out_dev: device pointer receiving the result; stream: cudaStream_t (NULL =
+ * default stream).  Queues the Gray-code form on `stream` and returns without waiting.
+ * All scratch lives in one fixed device array of 16.9 MB (16,924,928 bytes) inside the library, held
+ * by every GPU that loads the library until the process exits: no cudaMalloc, cudaFree or
+ * allocating library routine is called.  Limit: 20 <= n <= 36 (QB_ETOOBIG otherwise);
+ * up to 4096 candidate records (out_dev->status = QB_EOVERFLOW beyond); integer Q needs
+ * sum |Q_ij| < 2^53 (out_dev->status = QB_ERANGE otherwise).
+ * The first call on a device resolves the array's address (cudaGetSymbolAddress with that
+ * device current): make it before any stream capture.  Every call reuses the same array,
+ * so calls that overlap on the GPU race; serialise them. */
+int qb_solve_noalloc(int device, const double* q_dev, int32_t n, int32_t is_integer, int32_t prefix_bits,
+                     qb_noalloc_result* out_dev, void* stream);
 
 #ifdef __cplusplus
 }
