@@ -87,6 +87,7 @@ def load():
     L.qb_solve_batch.argtypes = [H, ctypes.POINTER(QbProblem), ctypes.c_int32, ctypes.POINTER(QbOptions),
                                  ctypes.POINTER(QbResult)]
     L.qb_autotune.argtypes = [H, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.qb_prefix_minima.argtypes = [H, ctypes.POINTER(QbProblem), ctypes.c_int32, ctypes.c_void_p]
     L.qb_solve_noalloc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                    ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
@@ -206,6 +207,20 @@ class Handle:
         if rc:
             _raise(rc, "qb_solve_batch")
         return [result_dict(res[i], probs[i].n) for i in range(len(Qs))]
+
+    def prefix_minima(self, Q: np.ndarray, prefix_bits: int = -1) -> np.ndarray:
+        """Per-prefix minimum energies in QBF's Gray visiting order (qb_prefix_minima)."""
+        p, keep = self._problem(Q)
+        n = p.n
+        A = n - min(n, 20) if prefix_bits < 0 else int(prefix_bits)
+        if A < 0 or A > 26:
+            raise ValueError(f"prefix_bits={prefix_bits} out of range for n={n}")
+        out = np.empty(1 << A, dtype=np.float64)
+        rc = load().qb_prefix_minima(self._h, ctypes.byref(p), int(prefix_bits), out.ctypes.data)
+        del keep
+        if rc:
+            _raise(rc, "qb_prefix_minima")
+        return out
 
     def autotune(self, n: int, dtype) -> str:
         f = ctypes.c_int32()

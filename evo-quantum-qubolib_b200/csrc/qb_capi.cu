@@ -68,6 +68,7 @@ struct HostBuf {
 
 constexpr double kTwo24 = 16777216.0;
 constexpr double kTwo53 = 9007199254740992.0;
+constexpr int kPrefixMinimaMaxA = 26;  // qb_prefix_minima: at most 2^26 prefixes (512 MiB of results)
 constexpr int kDefaultCap = 1 << 16;
 
 struct Plan {
@@ -643,6 +644,53 @@ int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, cons
     int rc = qb_solve(h, &problems[i], o, &r[i]);
     if (rc) return rc;
   }
+  return QB_OK;
+}
+
+int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, double* out) {
+  if (!h || !p || !out) return QB_EINVAL;
+  if (p->n < 1 || p->n > qb::kMaxN || !p->q || p->ldq < p->n || dtype_size(p->dtype) == 0) return QB_EINVAL;
+  const int n = p->n;
+  const int A = prefix_bits < 0 ? n - std::min(n, 20) : prefix_bits;
+  const int B = n - A;
+  if (A < 0 || A > kPrefixMinimaMaxA || B > qb::kExactMaxFree) return QB_EINVAL;
+  QB_CUDA(cudaSetDevice(h->device));
+  h->st = h->own;
+  h->pending = false;
+  h->kernels = 0;
+  h->h2d = h->d2h = 0;
+  std::vector<double> W;
+  double abs_sum = 0.0;
+  bool is_int = false;
+  int rc = load_problem(h, p, W, &abs_sum, &is_int);
+  if (rc) return rc;
+  if (abs_sum >= kTwo53) return QB_ERANGE;
+  rc = upload_W(h, W);
+  if (rc) return rc;
+  // one exact record per prefix value: the 2^B states whose first A variables spell it
+  qb::RecGeom geom{};
+  geom.kind = qb::kGeomBlock;
+  geom.n = n;
+  geom.fbits = B;
+  qb::TieRule rule{qb::kTieNatural, n, 0, 0, 0};
+  const qb::ProblemDev pd{n, static_cast<const double*>(h->W.p)};
+  const uint64_t count = 1ull << A;
+  QB_CUDA(h->exout.ensure(count * sizeof(qb::ExactOut)));
+  const size_t sm = qb::exact_smem_bytes(n, B);
+  QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const uint64_t maxg = 1u << 30;
+  for (uint64_t off = 0; off < count; off += maxg) {
+    const uint64_t g = std::min<uint64_t>(maxg, count - off);
+    qb::exact_records_kernel<<<(unsigned)g, qb::kExactThreads, sm, h->st>>>(
+        pd, rule, geom, nullptr, nullptr, (int64_t)count, (int64_t)off, static_cast<qb::ExactOut*>(h->exout.p) + off);
+    ++h->kernels;
+  }
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(h->hout.ensure(count * sizeof(qb::ExactOut)));
+  QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, count * sizeof(qb::ExactOut), cudaMemcpyDeviceToHost, h->st));
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
+  for (uint64_t i = 0; i < count; ++i) out[i] = eo[qb::gray64(i)].e;  // QBF's prefix visiting order
   return QB_OK;
 }
 

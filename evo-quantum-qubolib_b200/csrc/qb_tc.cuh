@@ -35,7 +35,9 @@
 //   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4)..+31 and the column quarter
 //               64*((w-4)/4)..+63 of every tile; it releases the accumulator stage as soon
 //               as its loads have landed, then reduces
-// Pipelines on mbarriers: 64 tile-parameter slots, 8 B stages, 2 accumulator stages.
+// Pipelines on mbarriers: 64 tile-parameter slots, 8 B stages, 2 accumulator stages.  One
+// tcgen05.commit per MMA (accumulator full); the MMA thread frees tile j-2's B stage and
+// parameter slot when the epilogue's release of tile j-2 lets it issue MMA j.
 // Every wait is bounded (%globaltimer): on timeout the waiting role raises an error flag,
 // the CTA drains and frees TMEM, and the host reports QB_ETIMEOUT.
 //
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
       mbar_init(&p_full[s], 1);
-      mbar_init(&p_empty[s], 1 + kTcEpiWarps);  // the tile's producer warp + every epilogue warp
+      mbar_init(&p_empty[s], 2);  // the tile's producer warp + the MMA thread (tile consumed)
     }
     for (int s = 0; s < kTcBStages; ++s) {
       mbar_init(&b_full[s], 1);
@@ -473,15 +475,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
              mbar_wait(&acc_empty[as], (uint32_t)(((j / kTcStages) & 1) ^ 1), abort_flag);
         if (!ok) break;
         tc_fence_after();
+        if (j >= (uint64_t)kTcStages) {
+          // every epilogue warp has released tile j-2 (it read that tile's parameters before
+          // its release, and MMA j-2 completed before the tile could be read): its B stage and
+          // parameter slot are free
+          const uint64_t jp = j - kTcStages;
+          mbar_arrive(&b_empty[jp % kTcBStages]);
+          mbar_arrive(&p_empty[jp % kTcParamSlots]);
+        }
         const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
         tc_mma(tmem + (uint32_t)as * (uint32_t)kTcN, adesc, bdesc);
-        tc_commit(&b_empty[bs]);
-        tc_commit(&acc_full[as]);
+        tc_commit(&acc_full[as]);  // one commit per MMA
         issued = j + 1;
       }
       if (issued) {  // let the last MMA finish before the CTA can release TMEM
         const uint64_t j = issued - 1;
-        mbar_wait(&b_empty[j % kTcBStages], (uint32_t)((j / kTcBStages) & 1), abort_flag);
+        mbar_wait(&acc_full[j % kTcStages], (uint32_t)((j / kTcStages) & 1), abort_flag);
       }
     }
     __syncwarp();
@@ -559,8 +568,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
 #pragma unroll
         for (int i = 0; i < 7; ++i) R = fmaf(ybit[i], sl.g[i], R);
       }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&p_empty[s]);
       ok = mbar_wait(&acc_full[as], (uint32_t)((j / kTcStages) & 1), abort_flag);
       if (!ok) break;
       tc_fence_after();

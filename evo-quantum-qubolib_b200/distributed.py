@@ -36,6 +36,26 @@ def _gather_best(res: dict, device):
     return best
 
 
+def combine_ranks(begin, finish, comm_device):
+    """The exchange of a sharded search, independent of how a shard is searched.
+
+    begin() searches this rank's share and returns its pass-1 minimum; finish(global_min)
+    re-evaluates the share's candidates against the global minimum and returns the share's
+    result dict (found, best_E, order_key, best_X_int).  The collectives run on tensors of
+    comm_device ("cuda:i" under NCCL, "cpu" under gloo).  Returns (this rank's result,
+    (E, key, X) of the global winner)."""
+    import torch
+    import torch.distributed as dist
+    lmin = begin()
+    t = torch.tensor([lmin], dtype=torch.float64, device=comm_device)
+    dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    res = finish(float(t.item()))
+    best = _gather_best(res, comm_device)
+    if best is None:
+        raise RuntimeError("no rank holds a minimising state")
+    return res, best
+
+
 def solve_sharded(Q: np.ndarray, form: str = "auto", tie_rule: str = "qbf", fixed_bits: int = 0,
                   prefix_bits: int = -1, device: int | None = None, Q_device_ptr: int | None = None) -> dict:
     """Exhaustive minimum of Q across all ranks of the default process group.
@@ -53,15 +73,13 @@ def solve_sharded(Q: np.ndarray, form: str = "auto", tie_rule: str = "qbf", fixe
     opts = dict(form=form, tie_rule=tie_rule, fixed_bits=fixed_bits, prefix_bits=prefix_bits, shard_index=rank,
                 shard_count=world, stream=stream)
     n = Q.shape[0]
-    if Q_device_ptr is not None:
-        lmin = h.solve_begin_device(Q_device_ptr, n, Q.dtype, **opts)
-    else:
-        lmin = h.solve_begin(Q, **opts)
-    t = torch.tensor([lmin], dtype=torch.float64, device=f"cuda:{device}")
-    dist.all_reduce(t, op=dist.ReduceOp.MIN)
-    res = h.solve_finish(float(t.item()), n)
-    best = _gather_best(res, f"cuda:{device}")
-    e, key, x = best
+
+    def begin():
+        if Q_device_ptr is not None:
+            return h.solve_begin_device(Q_device_ptr, n, Q.dtype, **opts)
+        return h.solve_begin(Q, **opts)
+
+    res, (e, key, x) = combine_ranks(begin, lambda gmin: h.solve_finish(gmin, n), f"cuda:{device}")
     out = dict(res)
     out.update(best_E=e, order_key=key, best_X_int=x,
                best_X=np.array([(x >> (n - 1 - i)) & 1 for i in range(n)], dtype=np.int32),

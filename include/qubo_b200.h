@@ -144,6 +144,14 @@ int qb_solve_finish(qb_handle* h, double global_min, qb_result* r);
 int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, const qb_options* o,
                    qb_result* r);
 
+/* Minimum energy of every A-bit prefix, in the order QBF's prefix loop visits them:
+ * out[i] = min over the last n - A variables of E(x) with the first A variables equal to
+ * the MSB-first bits of gray(i) = i ^ (i >> 1).  out holds 2^A doubles (host memory).
+ * prefix_bits = A (-1 = QBF default n - min(n, 20)); A <= 26 and n - A <= 40.  Energies
+ * are exact FP64 sums (integer Q exact).  Replaces the energy_arr metric that QBF records
+ * per prefix in update_global_minima (src/qubo_lib/solvers/qbf.py:395-412, 342-351). */
+int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, double* out);
+
 /* Pick the fastest form for problems of n variables and dtype by timing candidate kernel
  * configurations on the handle's device; the choice is cached in the handle and used by
  * QB_FORM_AUTO.  *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond

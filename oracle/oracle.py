@@ -231,3 +231,27 @@ def qbf1_numpy(Q) -> dict:
         row = E[p << 18:(p + 1) << 18]
         X = (p << 18) | int(np.flatnonzero(row == emin)[0])
     return {"best_E": int(round(E[X])), "best_X_int": X, "best_X": [(X >> (n - 1 - i)) & 1 for i in range(n)]}
+
+
+def prefix_minima_numpy(Q, A: int) -> np.ndarray:
+    """QBF's energy_arr restated: entry i is the smallest energy over all suffixes of the
+    prefix visited at Gray step i, i.e. the A MSB-first bits of gray(i)
+    (src/qubo_lib/solvers/qbf.py:291-325 visiting order, :395-412 one value per step).
+    FP64; exact for integer Q.  n <= 24."""
+    E = all_energies(Q)
+    n = np.asarray(Q).shape[0]
+    per_prefix = E.reshape(1 << A, 1 << (n - A)).min(axis=1)
+    i = np.arange(1 << A)
+    return per_prefix[i ^ (i >> 1)]
+
+
+def parallel_energy_arr_numpy(Q, k: int, A_sub: int) -> np.ndarray:
+    """Parallel(QBF)'s energy_arr restated: tasks in task order (one worker), each task's
+    per-prefix minima of its ReducedProblem plus the task's prefix_E, which is the full
+    problem's energy (src/qubo_lib/solvers/parallel.py:250-270, 145-157)."""
+    E = all_energies(Q)
+    n = np.asarray(Q).shape[0]
+    B = n - k - A_sub
+    per = E.reshape(1 << k, 1 << A_sub, 1 << B).min(axis=2)
+    i = np.arange(1 << A_sub)
+    return per[:, i ^ (i >> 1)].reshape(-1)

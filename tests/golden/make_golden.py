@@ -4,6 +4,7 @@ Run in a container that holds the reference source (cloud-ru-tech/evo-quantum-qu
 under /root/reference:
 
     python tests/golden/make_golden.py            # all fixtures (a few minutes)
+    python tests/golden/make_golden.py metrics    # metrics.json only
 
 The reference is imported from /root/reference/src with the test-only stubs in
 tests/golden/refstub (jsonpickle and ortools are not installed; neither is on the search
@@ -147,7 +148,42 @@ def small_cases() -> list:
     return cases
 
 
+def metrics_fixture():
+    """energy_arr (use_metrics='all') of QBF and of Parallel(QBF) with one worker, which
+    visits the tasks in task order."""
+    rng = np.random.default_rng(515)
+    recs = []
+    for name, A in (("i32sym_n12_A4", 4), ("i16asym_n14_A5", 5), ("f32_n12_A3", 3), ("f64_n10_A4", 4),
+                    ("i32sym_n9_A4", 4)):
+        n = int(name.split("_n")[1].split("_")[0])
+        if name.startswith("i32sym"):
+            U = rng.integers(-30, 31, (n, n)).astype(np.int32)
+            Q = np.triu(U) + np.triu(U, 1).T
+        elif name.startswith("i16"):
+            Q = rng.integers(-30, 31, (n, n)).astype(np.int16)
+        elif name.startswith("f32"):
+            Q = rng.standard_normal((n, n)).astype(np.float32)
+        else:
+            Q = rng.standard_normal((n, n))
+        sol = QBF().solve(Just_Q(Q), A=A, use_metrics="all")
+        recs.append({"name": name, "solver": "QBF", "Q": enc_q(Q), "A": A, "best_E": float(sol.best_E),
+                     "energy_arr": [float(v) for v in sol.metrics[0]["energy_arr"]],
+                     "time_arr_len": int(len(sol.metrics[0]["time_arr"]))})
+    for name, n, splits, A in (("par_i32_n12_k4_A3", 12, 4, 3), ("par_i32_n11_k2_A0", 11, 2, 0)):
+        U = rng.integers(-30, 31, (n, n)).astype(np.int32)
+        Q = np.triu(U) + np.triu(U, 1).T
+        sol = Parallel(base_solver=QBF, splits_cnt=splits, devices=["cpu"]).solve(Just_Q(Q), A=A, use_metrics="all")
+        recs.append({"name": name, "solver": "Parallel", "splits_cnt": splits, "Q": enc_q(Q), "A": A,
+                     "best_E": float(sol.best_E), "energy_arr": [float(v) for v in sol.metrics[0]["energy_arr"]]})
+    json.dump({"source": "reference QBF / Parallel(QBF, devices=['cpu']) with use_metrics='all'", "cases": recs},
+              open(os.path.join(HERE, "metrics.json"), "w"))
+    print("metrics", len(recs))
+
+
 def main():
+    if sys.argv[1:] == ["metrics"]:
+        metrics_fixture()
+        return
     out = {}
     # ------------------------------------------------------------------ QBF small
     recs = []
@@ -304,6 +340,7 @@ def main():
     cfg["cfg5_subset"] = batch
     json.dump(cfg, open(os.path.join(HERE, "configs.json"), "w"))
     print("configs done")
+    metrics_fixture()
 
 
 if __name__ == "__main__":
