@@ -1,8 +1,6 @@
 """Build libqubo_b200.so in-tree for sm_100a (nvcc cross-compiles without a GPU).
 
-    python evo-quantum-qubolib_b200/build.py [--force] [--debug]
-
---debug adds -DQB_CHECK (bounds checks that record a bad index and skip the access).
+    python evo-quantum-qubolib_b200/build.py [--force]
 """
 from __future__ import annotations
 
@@ -35,10 +33,10 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps())
 
 
-def build(force: bool = False, debug: bool = False, verbose: bool = False) -> str:
-    if not force and not debug and up_to_date():
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and up_to_date():
         return OUT
-    cmd = [NVCC] + FLAGS + (["-DQB_CHECK"] if debug else []) + sources() + ["-o", OUT]
+    cmd = [NVCC] + FLAGS + sources() + ["-o", OUT]
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
         sys.stderr.write(p.stdout + p.stderr)
@@ -49,4 +47,4 @@ def build(force: bool = False, debug: bool = False, verbose: bool = False) -> st
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, debug="--debug" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True))
