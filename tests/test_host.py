@@ -136,3 +136,14 @@ def test_c_abi_host_only_calls():
     for s in range(9):
         assert L.qb_strerror(s)
     assert b"no-allocation" in L.qb_strerror(8)
+
+
+def test_config_generators_match_reference_inputs():
+    from qubo_b200 import configs
+    cfg = load_golden("configs.json")
+    np.testing.assert_array_equal(configs.random_f32_n20(), dec_q(cfg["cfg1"]["Q"]))
+    np.testing.assert_array_equal(configs.random_i16_n32(), dec_q(cfg["cfg2"]["Q"]))
+    np.testing.assert_array_equal(configs.tsp6_int(), dec_q(cfg["cfg3"]["Q"]))
+    np.testing.assert_array_equal(configs.maxcut_er(), dec_q(cfg["cfg4"]["Q"]))
+    for b in cfg["cfg5_subset"]:
+        np.testing.assert_array_equal(configs.batch_instance(b["index"], seed=1000), dec_q(b["Q"]))
