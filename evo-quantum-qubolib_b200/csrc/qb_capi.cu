@@ -11,6 +11,7 @@
 // Only pass 1 touches all 2^n states.  For integer Q inside the fp32-exact range the
 // selection keeps exactly the records that hold a minimal state.
 #include "../../include/qubo_b200.h"
+#include "qb_batch.cuh"
 #include "qb_common.cuh"
 #include "qb_exact.cuh"
 #include "qb_gray.cuh"
@@ -96,6 +97,7 @@ struct qb_handle_s {
   cudaStream_t own = nullptr;
   cudaStream_t st = nullptr;
   DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
+  DevBuf bat[10];  // qb_solve_batch: W, insts, gtab items, unit items, gray ids, cands, out, G tables, records, minima
   HostBuf hW, hmisc, hout;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // 4, 5: main kernel
   int64_t h2d = 0, d2h = 0;  // bytes copied by the current call
@@ -406,6 +408,7 @@ int qb_handle_destroy(qb_handle* h) {
   h->misc.release();
   h->exout.release();
   h->tcscratch.release();
+  for (auto& b : h->bat) b.release();
   h->hW.release();
   h->hmisc.release();
   h->hout.release();
@@ -638,13 +641,234 @@ int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* 
   return rc;
 }
 
-int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, const qb_options* o, qb_result* r) {
-  if (!h || !problems || !o || !r || count < 0) return QB_EINVAL;
-  for (int32_t i = 0; i < count; ++i) {
+}  // extern "C"
+
+namespace {
+
+constexpr int kBatchMaxN = 36;            // larger problems are solved one by one
+constexpr uint64_t kBatchGtabChunk = 1024;  // G-table steps per CTA
+
+template <class T>
+int upload_vec(qb_handle* h, DevBuf& d, const std::vector<T>& v) {
+  const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+  QB_CUDA(d.ensure(bytes));
+  if (!v.empty()) {
+    QB_CUDA(cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
+    h->h2d += (int64_t)(v.size() * sizeof(T));
+  }
+  return QB_OK;
+}
+
+int batch_loop(qb_handle* h, const qb_problem* problems, const std::vector<int32_t>& ids, const qb_options* o,
+               qb_result* r) {
+  for (int32_t i : ids) {
     int rc = qb_solve(h, &problems[i], o, &r[i]);
     if (rc) return rc;
   }
   return QB_OK;
+}
+
+// The batched search of problems[ids] (all 1 <= n <= kBatchMaxN), QB_TIE_QBF with no task
+// bits or QB_TIE_NATURAL.
+int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_t>& ids, const qb_options* o,
+              qb_result* r, bool* overflow) {
+  *overflow = false;
+  const int m = (int)ids.size();
+  if (!m) return QB_OK;
+  std::vector<qb::BatchInst> insts(m);
+  std::vector<double> Wall;
+  std::vector<qb::BatchItem> gitems, uitems;
+  std::vector<uint32_t> gray_ids;
+  std::vector<qb::BatchCand> pre;
+  uint64_t gtab_total = 0, rec_total = 0;
+  size_t sm_gtab = 0, sm_gray = 0, sm_exact = 0;
+  for (int j = 0; j < m; ++j) {
+    const qb_problem* p = &problems[ids[j]];
+    std::vector<double> W;
+    double abs_sum = 0.0;
+    bool is_int = false;
+    int rc = load_problem(h, p, W, &abs_sum, &is_int);
+    if (rc) return rc;
+    if (abs_sum >= kTwo53) return QB_ERANGE;
+    const int n = p->n;
+    qb::BatchInst& I = insts[j];
+    memset(&I, 0, sizeof(I));
+    I.n = n;
+    I.is_int = is_int ? 1 : 0;
+    I.natural = o->tie_rule == QB_TIE_NATURAL ? 1 : 0;
+    I.A = o->prefix_bits < 0 ? n - std::min(n, 20) : o->prefix_bits;
+    if (I.A > n) return QB_EINVAL;
+    I.B = n - I.A;
+    I.w_off = Wall.size();
+    Wall.insert(Wall.end(), W.begin(), W.end());
+    int free_bits;
+    if (n >= 20) {
+      I.kind = qb::kBatchGray;
+      I.b = std::max(13, n - 16);
+      I.a = n - I.b;
+      I.cbbits = I.b - 13;
+      I.sbits = std::min(I.a, std::max(5, n - 34));
+      const int ubits = std::min(I.a, std::max(7, std::max(I.sbits, std::min(I.a, I.a + I.cbbits - 11))));
+      I.gubits = ubits - I.sbits;
+      const uint64_t units = 1ull << (I.a - ubits + I.cbbits);
+      I.nrec = units << (I.gubits + 3);
+      I.eps = (is_int && abs_sum < kTwo24) ? 0.0 : qb::gray_error_bound(abs_sum);
+      I.gtab_off = gtab_total;
+      gtab_total += (1ull << I.a) * 32;
+      I.rec_off = rec_total;
+      rec_total += I.nrec;
+      for (uint64_t lo = 0; lo < (1ull << I.a); lo += kBatchGtabChunk)
+        gitems.push_back(qb::BatchItem{(uint32_t)j, 0u, lo, std::min<uint64_t>(lo + kBatchGtabChunk, 1ull << I.a)});
+      for (uint64_t u = 0; u < units; ++u) uitems.push_back(qb::BatchItem{(uint32_t)j, 0u, u, u + 1});
+      gray_ids.push_back((uint32_t)j);
+      sm_gtab = std::max(sm_gtab, qb::gray_gtab_smem(n, I.a));
+      sm_gray = std::max(sm_gray, qb::gray_pass1_smem(n, I.a));
+      free_bits = I.sbits + 10;
+    } else {
+      I.kind = qb::kBatchExact;
+      I.fbits = std::min(n, 16);
+      for (uint64_t rid = 0; rid < (1ull << (n - I.fbits)); ++rid) pre.push_back(qb::BatchCand{(uint32_t)j, 0u, rid});
+      free_bits = I.fbits;
+    }
+    sm_exact = std::max(sm_exact, qb::exact_smem_bytes(n, free_bits));
+  }
+  // candidate list: the small problems' records first, then room for the Gray problems'
+  const int prefilled = (int)pre.size();
+  const int cap = prefilled + std::max(4096, 8 * (int)gray_ids.size());
+  // device buffers
+  DevBuf* B = h->bat;
+  int rc;
+  if ((rc = upload_vec(h, B[0], Wall))) return rc;
+  if ((rc = upload_vec(h, B[1], insts))) return rc;
+  if ((rc = upload_vec(h, B[2], gitems))) return rc;
+  if ((rc = upload_vec(h, B[3], uitems))) return rc;
+  if ((rc = upload_vec(h, B[4], gray_ids))) return rc;
+  QB_CUDA(B[5].ensure((size_t)cap * sizeof(qb::BatchCand)));  // room first: ensure() may reallocate
+  if ((rc = upload_vec(h, B[5], pre))) return rc;
+  QB_CUDA(B[6].ensure((size_t)cap * sizeof(qb::ExactOut)));
+  QB_CUDA(B[7].ensure(std::max<uint64_t>(gtab_total, 4) * sizeof(float)));
+  QB_CUDA(B[8].ensure(std::max<uint64_t>(rec_total, 4) * sizeof(float)));
+  // minima: emin[m], kmin[m] (uint64), pass1_min[m] (float), cand_count (int)
+  const size_t mb = (size_t)m * 8;
+  QB_CUDA(B[9].ensure(2 * mb + (size_t)m * 4 + 16));
+  uint64_t* emin = static_cast<uint64_t*>(B[9].p);
+  uint64_t* kmin = emin + m;
+  float* p1min = reinterpret_cast<float*>(kmin + m);
+  int* ccount = reinterpret_cast<int*>(static_cast<char*>(B[9].p) + 2 * mb + (size_t)m * 4);
+  QB_CUDA(cudaMemsetAsync(B[9].p, 0xff, 2 * mb, h->st));
+  QB_CUDA(h->hmisc.ensure(64));
+  *static_cast<int*>(h->hmisc.p) = prefilled;
+  QB_CUDA(cudaMemcpyAsync(ccount, h->hmisc.p, sizeof(int), cudaMemcpyHostToDevice, h->st));
+  h->h2d += (int64_t)sizeof(int);
+  const double* dW = static_cast<const double*>(B[0].p);
+  const qb::BatchInst* dI = static_cast<const qb::BatchInst*>(B[1].p);
+  qb::BatchCand* dC = static_cast<qb::BatchCand*>(B[5].p);
+  qb::ExactOut* dO = static_cast<qb::ExactOut*>(B[6].p);
+  QB_CUDA(cudaEventRecord(h->ev[0], h->st));
+  QB_CUDA(cudaEventRecord(h->ev[4], h->st));
+  if (!gray_ids.empty()) {
+    QB_CUDA(cudaFuncSetAttribute(qb::batch_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gtab));
+    qb::batch_gtab_kernel<<<(unsigned)gitems.size(), 256, sm_gtab, h->st>>>(
+        dI, static_cast<const qb::BatchItem*>(B[2].p), dW, static_cast<float*>(B[7].p));
+    QB_CUDA(cudaFuncSetAttribute(qb::batch_gray_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gray));
+    qb::batch_gray_kernel<<<(unsigned)uitems.size(), qb::kGrayThreads, sm_gray, h->st>>>(
+        dI, static_cast<const qb::BatchItem*>(B[3].p), dW, static_cast<const float*>(B[7].p),
+        static_cast<float*>(B[8].p));
+    h->kernels += 2;
+  }
+  QB_CUDA(cudaEventRecord(h->ev[5], h->st));
+  QB_CUDA(cudaEventRecord(h->ev[1], h->st));
+  QB_CUDA(cudaEventRecord(h->ev[2], h->st));
+  if (!gray_ids.empty()) {
+    qb::batch_select_kernel<<<(unsigned)gray_ids.size(), 256, 0, h->st>>>(
+        dI, static_cast<const uint32_t*>(B[4].p), static_cast<const float*>(B[8].p), dC, ccount, cap, p1min, emin,
+        kmin);
+    ++h->kernels;
+  }
+  QB_CUDA(cudaFuncSetAttribute(qb::batch_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_exact));
+  qb::batch_exact_kernel<<<(unsigned)cap, qb::kExactThreads, sm_exact, h->st>>>(dI, dW, dC, ccount, cap, dO, emin);
+  qb::batch_key_kernel<<<(unsigned)std::min<int>((cap + 255) / 256, h->sm_count * 4), 256, 0, h->st>>>(
+      dC, ccount, cap, dO, emin, kmin);
+  h->kernels += 2;
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(cudaEventRecord(h->ev[3], h->st));
+  QB_CUDA(h->hout.ensure(B[9].cap));
+  QB_CUDA(cudaMemcpyAsync(h->hout.p, B[9].p, 2 * mb + (size_t)m * 4 + sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  h->d2h += (int64_t)(2 * mb + (size_t)m * 4 + sizeof(int));
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  const uint64_t* he = static_cast<const uint64_t*>(h->hout.p);
+  const uint64_t* hk = he + m;
+  const float* hp = reinterpret_cast<const float*>(hk + m);
+  const int got = *reinterpret_cast<const int*>(reinterpret_cast<const char*>(h->hout.p) + 2 * mb + (size_t)m * 4);
+  if (got > cap) {
+    *overflow = true;
+    return QB_OK;
+  }
+  float p1 = 0.f, p2 = 0.f, km = 0.f;
+  QB_CUDA(cudaEventElapsedTime(&p1, h->ev[0], h->ev[1]));
+  QB_CUDA(cudaEventElapsedTime(&p2, h->ev[2], h->ev[3]));
+  QB_CUDA(cudaEventElapsedTime(&km, h->ev[4], h->ev[5]));
+  for (int j = 0; j < m; ++j) {
+    const qb::BatchInst& I = insts[j];
+    qb_result& R = r[ids[j]];
+    memset(&R, 0, sizeof(R));
+    if (he[j] == ~0ull || hk[j] == ~0ull) {
+      R.status = QB_ECUDA;
+      return QB_ECUDA;
+    }
+    const uint64_t key = hk[j];
+    const uint64_t x = I.natural ? key : ((qb::gray64(key >> I.B) << I.B) | (key & qb::mask64(I.B)));
+    R.best_x = x;
+    R.best_e = qb::unord_f64(he[j]);
+    R.best_e_int = I.is_int ? (int64_t)llround(R.best_e) : 0;
+    R.order_key = key;
+    R.pass1_min = I.kind == qb::kBatchGray ? (double)hp[j] : R.best_e;
+    R.err_bound = I.eps;
+    R.states = (int64_t)1 << I.n;
+    R.form_used = I.kind == qb::kBatchGray ? QB_FORM_GRAY : QB_FORM_EXACT;
+    R.is_integer = I.is_int;
+    R.found = 1;
+    R.status = QB_OK;
+    R.pass1_ms = p1;
+    R.pass2_ms = p2;
+    R.kernels = h->kernels;
+    R.kernel_ms = km;
+    R.h2d_bytes = h->h2d;
+    R.d2h_bytes = h->d2h;
+  }
+  return QB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, const qb_options* o, qb_result* r) {
+  if (!h || !problems || !o || !r || count < 0) return QB_EINVAL;
+  std::vector<int32_t> batched, single;
+  const bool rule_ok = (o->tie_rule == QB_TIE_QBF && o->fixed_bits == 0) || o->tie_rule == QB_TIE_NATURAL;
+  const bool form_ok = o->form == QB_FORM_AUTO || o->form == QB_FORM_GRAY;
+  for (int32_t i = 0; i < count; ++i) {
+    const qb_problem* p = &problems[i];
+    if (p->n < 1 || p->n > qb::kMaxN || !p->q || p->ldq < p->n || dtype_size(p->dtype) == 0) return QB_EINVAL;
+    if (rule_ok && form_ok && o->shard_count <= 1 && p->n <= kBatchMaxN)
+      batched.push_back(i);
+    else
+      single.push_back(i);
+  }
+  if (!batched.empty()) {
+    QB_CUDA(cudaSetDevice(h->device));
+    h->st = o->stream ? static_cast<cudaStream_t>(o->stream) : h->own;
+    h->pending = false;
+    h->kernels = 0;
+    h->h2d = h->d2h = 0;
+    bool overflow = false;
+    int rc = batch_run(h, problems, batched, o, r, &overflow);
+    if (rc) return rc;
+    if (overflow) single.insert(single.end(), batched.begin(), batched.end());  // too many candidates
+  }
+  std::sort(single.begin(), single.end());
+  return batch_loop(h, problems, single, o, r);
 }
 
 int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, double* out) {

@@ -45,19 +45,12 @@ __device__ __forceinline__ bool lex_less(double e1, uint64_t k1, double e2, uint
   return e1 < e2 || (e1 == e2 && k1 < k2);
 }
 
-// rec_ids: candidate record indices (nullptr: record = rec_offset + blockIdx.x).
-// count_ptr: number of valid entries (nullptr: count_static).
-__global__ void __launch_bounds__(kExactThreads)
-exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restrict__ rec_ids,
-                     const int* __restrict__ count_ptr, int64_t count_static, int64_t rec_offset,
-                     ExactOut* __restrict__ out) {
-  extern __shared__ double smem_d[];
+// One CTA (kExactThreads threads) evaluates record rid exactly and thread 0 writes the
+// record's lexicographic minimum to *out_slot.  smem_d: exact_smem_bytes(n, f) of dynamic
+// shared memory.
+__device__ __forceinline__ void exact_record_body(const ProblemDev& P, const TieRule& R, const RecGeom& G,
+                                                  uint64_t rid, ExactOut* __restrict__ out_slot, double* smem_d) {
   const int n = P.n;
-  const int64_t slot = (int64_t)blockIdx.x + (rec_ids ? rec_offset : 0);
-  const int64_t count = count_ptr ? (int64_t)(*count_ptr) : count_static;
-  if (slot >= count) return;
-  const uint64_t rid = rec_ids ? rec_ids[slot] : (uint64_t)(rec_offset + blockIdx.x);
-
   double* Ws = smem_d;                       // n*n
   double* Wl = Ws + n * n;                   // L*L couplings among low free variables
   __shared__ int pos[kExactMaxFree];         // free bit positions, ascending
@@ -161,8 +154,22 @@ exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restr
         best_k = red_k[w];
         best_x = red_x[w];
       }
-    out[slot] = ExactOut{best_e, best_k, best_x};
+    *out_slot = ExactOut{best_e, best_k, best_x};
   }
+}
+
+// rec_ids: candidate record indices (nullptr: record = rec_offset + blockIdx.x).
+// count_ptr: number of valid entries (nullptr: count_static).
+__global__ void __launch_bounds__(kExactThreads)
+exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restrict__ rec_ids,
+                     const int* __restrict__ count_ptr, int64_t count_static, int64_t rec_offset,
+                     ExactOut* __restrict__ out) {
+  extern __shared__ double smem_d[];
+  const int64_t slot = (int64_t)blockIdx.x + (rec_ids ? rec_offset : 0);
+  const int64_t count = count_ptr ? (int64_t)(*count_ptr) : count_static;
+  if (slot >= count) return;
+  const uint64_t rid = rec_ids ? rec_ids[slot] : (uint64_t)(rec_offset + blockIdx.x);
+  exact_record_body(P, R, G, rid, out + slot, smem_d);
 }
 
 inline size_t exact_smem_bytes(int n, int f) {

@@ -41,9 +41,11 @@ struct GrayParams {
 // per-state error bound of the fp32 path (see the header comment)
 inline double gray_error_bound(double abs_sum) { return 300.0 * abs_sum * 5.9604644775390625e-08; }
 
-// G(p)[c] for every Gray step i: one warp per step, lane = c.
-__global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__ gtab) {
-  extern __shared__ double gtab_smem[];
+// G(p)[c] for Gray steps i in [i_begin, i_end): one warp per step (warp w of the CTA takes
+// steps i_begin + first + w, + stride, ...), lane = c.  smem: gray_gtab_smem(n, a).
+__device__ __forceinline__ void gray_gtab_body(const ProblemDev& P, int a, float* __restrict__ gtab,
+                                               uint64_t i_begin, uint64_t i_end, uint64_t first, uint64_t stride,
+                                               double* gtab_smem) {
   const int n = P.n;
   double* Ws = gtab_smem;      // n*n
   double* beta = Ws + n * n;   // a * 32
@@ -58,9 +60,7 @@ __global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__
   }
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const uint64_t nsteps = 1ull << a;
-  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-  for (uint64_t i = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nsteps; i += warps) {
+  for (uint64_t i = i_begin + first + (threadIdx.x >> 5); i < i_end; i += stride) {
     const uint64_t p = gray64(i);
     // E_pre(p): lane handles prefix variables lane and lane + 32
     double ep = 0.0;
@@ -79,6 +79,13 @@ __global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__
   }
 }
 
+__global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__ gtab) {
+  extern __shared__ double gtab_smem[];
+  (void)b;
+  gray_gtab_body(P, a, gtab, 0, 1ull << a, (uint64_t)blockIdx.x * (blockDim.x >> 5),
+                 (uint64_t)gridDim.x * (blockDim.x >> 5), gtab_smem);
+}
+
 inline size_t gray_gtab_smem(int n, int a) { return (size_t)(n * n + a * 32) * sizeof(double); }
 
 // shared-memory carve-out, in this order so that the float4-read staging buffer sits at
@@ -91,8 +98,8 @@ inline size_t gray_pass1_smem(int n, int a) {
          + (size_t)a * kGrayThreads * sizeof(float);  // alpha (fp32, per step)
 }
 
-__global__ void __launch_bounds__(kGrayThreads, 2) gray_pass1_kernel(GrayParams g) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// One CTA searches work unit g.unit_begin + unit_local and writes its records.
+__device__ __forceinline__ void gray_unit_body(const GrayParams& g, uint64_t unit_local, unsigned char* smem_raw) {
   const int n = g.P.n, a = g.a, b = g.b;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   float* gbuf = reinterpret_cast<float*>(smem_raw);
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(kGrayThreads, 2) gray_pass1_kernel(GrayParams 
   double* Ws = alpha_d + a * kGrayThreads;
   float* alpha_f = reinterpret_cast<float*>(Ws + n * n);
 
-  const uint64_t unit = g.unit_begin + blockIdx.x;
+  const uint64_t unit = g.unit_begin + unit_local;
   const uint64_t cb = unit & mask64(g.cbbits);
   const uint64_t chunk = unit >> g.cbbits;
   const int ubits = g.gubits + g.sbits;
@@ -234,6 +241,11 @@ __global__ void __launch_bounds__(kGrayThreads, 2) gray_pass1_kernel(GrayParams 
     }
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(kGrayThreads, 2) gray_pass1_kernel(GrayParams g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  gray_unit_body(g, blockIdx.x, smem_raw);
 }
 
 }  // namespace qb

@@ -134,6 +134,32 @@ class QBF(SolverABC):
         self.timer.pick_time("search")
         return self._pack(problem, res, kwargs)
 
+    def solve_batch(self, problems, **kwargs) -> list:
+        """Solve many independent problems in one batched GPU search (qb_solve_batch) and
+        return one Solution per problem, each the one ``solve(problem, **kwargs)`` returns.
+        Problems with up to 36 variables share six kernel launches in total; larger ones are
+        solved one by one.  An addition: the reference solves one problem per call."""
+        self.check_obsolete_args(**kwargs)
+        if "B" in kwargs or "use_mem_GB" in kwargs:  # the split would differ per problem size
+            return [QBF().solve(p, **kwargs) for p in problems]
+        self.kwargs = kwargs
+        self.json_str = _json.encode(kwargs, indent=4)
+        dev = self.parse_device_arg(**kwargs)
+        stream = _torch_stream(dev)
+        self.timer = PerformanceTimer(use_gpu=True)
+        Qs = [np.asarray(p.build_Q_matrix(use_gpu=False)) for p in problems]
+        self.timer.pick_time("build_Q")
+        results = _lib.handle(dev).solve_batch(Qs, form=kwargs.get("form", "auto"), tie_rule="qbf", fixed_bits=0,
+                                               prefix_bits=int(kwargs.get("A", -1)), stream=stream)
+        self.timer.pick_time("search")
+        out = []
+        for problem, Q, res in zip(problems, Qs, results):
+            self.N = problem.N
+            self.Q = Q
+            self.A, self.B = QBF.define_chunk_size(N=self.N, **kwargs)
+            out.append(self._pack(problem, res, kwargs))
+        return out
+
     def _pack(self, problem, res, kwargs) -> Solution:
         best_X = res["best_X"]
         sol = Solution(self.N, 2 ** self.A, 1, problem.to_json(), self.json_str)

@@ -1,0 +1,112 @@
+"""qb_solve_batch (QBF.solve_batch): many problems of uneven size in one batched search,
+each answer equal to the single-problem answer and to the oracle's (bit-exact for integer
+Q, FP64 argmin within 1e-9 relative for float Q)."""
+import numpy as np
+import pytest
+
+import oracle
+import qubo_b200  # noqa: F401
+from conftest import bits_to_int, dec_q, load_golden
+from qubo_b200 import _lib, configs
+from qubo_b200.problems import Just_Q
+from qubo_b200.solvers import QBF
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed(seed, count):
+    rng = np.random.default_rng(seed)
+    Qs = []
+    for i in range(count):
+        n = int(rng.integers(1, 27))
+        kind = i % 4
+        if kind == 0:
+            U = rng.integers(-60, 61, (n, n)).astype(np.int32)
+            Qs.append((np.triu(U) + np.triu(U, 1).T).astype(np.int32))
+        elif kind == 1:
+            Qs.append(rng.integers(-9, 10, (n, n)).astype(np.int16))
+        elif kind == 2:
+            Qs.append(rng.standard_normal((n, n)).astype(np.float32))
+        else:
+            G = rng.standard_normal((n, n))
+            Qs.append((G + G.T) / 2)
+    return Qs
+
+
+def _check(Q, r):
+    ref = oracle.qbf_port(Q)
+    assert r["best_X_int"] == ref["best_X_int"], (Q.shape, Q.dtype, r, ref)
+    if np.issubdtype(Q.dtype, np.integer):
+        assert r["best_E"] == ref["best_E"]
+    else:
+        assert abs(r["best_E"] - ref["best_E"]) <= 1e-9 * max(1.0, abs(ref["best_E"]))
+
+
+def test_batch_mixed_sizes_and_dtypes(cuda_ok):
+    Qs = _mixed(3, 96)
+    res = _lib.handle(0).solve_batch(Qs)
+    assert len(res) == len(Qs)
+    for Q, r in zip(Qs, res):
+        _check(Q, r)
+
+
+def test_batch_twice_and_matches_single_calls(cuda_ok):
+    h = _lib.handle(0)
+    Qs = _mixed(4, 40)
+    a = h.solve_batch(Qs)
+    b = h.solve_batch(Qs[::-1])[::-1]
+    for Q, ra, rb in zip(Qs, a, b):
+        rs = h.solve(Q, form="auto")
+        assert ra["best_X_int"] == rb["best_X_int"] == rs["best_X_int"]
+        assert ra["best_E"] == rb["best_E"]
+        assert abs(ra["best_E"] - rs["best_E"]) <= 1e-9 * max(1.0, abs(rs["best_E"]))
+
+
+def test_batch_ties_follow_the_split(cuda_ok):
+    rng = np.random.default_rng(8)
+    Qs = [rng.integers(-2, 3, (n, n)).astype(np.int32) for n in (12, 18, 22, 25)]
+    for A in (0, 5, 9):
+        res = _lib.handle(0).solve_batch(Qs, prefix_bits=A)
+        for Q, r in zip(Qs, res):
+            ref = oracle.qbf_port(Q, A=A)
+            assert (r["best_X_int"], r["best_E"]) == (ref["best_X_int"], ref["best_E"])
+
+
+def test_batch_natural_rule_and_large_member(cuda_ok):
+    rng = np.random.default_rng(9)
+    Qs = [rng.integers(-3, 4, (n, n)).astype(np.int32) for n in (10, 21, 37)]
+    res = _lib.handle(0).solve_batch(Qs, tie_rule="natural")
+    for Q, r in zip(Qs, res):
+        single = _lib.handle(0).solve(Q, tie_rule="natural")
+        assert (r["best_X_int"], r["best_E"]) == (single["best_X_int"], single["best_E"])
+
+
+def test_batch_empty_and_zero_matrices(cuda_ok):
+    assert _lib.handle(0).solve_batch([]) == []
+    res = _lib.handle(0).solve_batch([np.zeros((n, n), np.int32) for n in (3, 20, 26)])
+    for r in res:
+        assert r["best_E"] == 0 and r["best_X_int"] == 0
+
+
+def test_solver_batch_cfg5_subset_against_reference(cuda_ok):
+    cases = load_golden("configs.json")["cfg5_subset"]
+    probs = [Just_Q(dec_q(c["Q"])) for c in cases]
+    sols = QBF().solve_batch(probs, device="cuda")
+    for c, p, sol in zip(cases, probs, sols):
+        Q = p.build_Q_matrix()
+        x = bits_to_int("".join(map(str, sol.best_X)))
+        ref = oracle.qbf_port(Q)
+        assert x == ref["best_X_int"]
+        assert abs(float(sol.best_E) - ref["best_E"]) <= 1e-9 * max(1.0, abs(ref["best_E"]))
+        assert sol.solver_class == "QBF" and sol.epochs_cnt == 2 ** sol_A(p.N)
+
+
+def sol_A(n):
+    return n - min(n, 20)
+
+
+def test_batch_cfg5_sample_of_4096(cuda_ok):
+    Qs = [configs.batch_instance(i) for i in range(0, 4096, 128)]
+    res = _lib.handle(0).solve_batch(Qs)
+    for Q, r in zip(Qs, res):
+        _check(Q, r)
