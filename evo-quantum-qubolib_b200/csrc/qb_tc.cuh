@@ -31,13 +31,14 @@
 //               publishes E_T(t), t^T W_TY and t^T W_TU of its tile
 //   warp 1      TMEM allocation and MMA issue (one elected thread)
 //   warps 2-3   B producers, alternate tiles: C_t(u) digits into the B stage (generic
-//               stores + proxy fence)
+//               stores + proxy fence) and the 128 row terms R_t(y) beside it
 //   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4)..+31 and the column quarter
 //               64*((w-4)/4)..+63 of every tile; it releases the accumulator stage as soon
 //               as its loads have landed, then reduces
-// Pipelines on mbarriers: 64 tile-parameter slots, 8 B stages, 2 accumulator stages.  One
-// tcgen05.commit per MMA (accumulator full); the MMA thread frees tile j-2's B stage and
-// parameter slot when the epilogue's release of tile j-2 lets it issue MMA j.
+// Pipelines on mbarriers: 64 tile-parameter slots (walk -> producers), 8 B stages
+// (producers -> MMA and epilogue), 2 accumulator stages.  One tcgen05.commit per MMA
+// (accumulator full); the MMA thread frees tile j-2's B stage when the epilogue's release
+// of tile j-2 lets it issue MMA j.
 // Every wait is bounded (%globaltimer): on timeout the waiting role raises an error flag,
 // the CTA drains and frees TMEM, and the host reports QB_ETIMEOUT.
 //
@@ -61,6 +62,7 @@ constexpr int kTcParamSlots = 64;
 constexpr int kTcBStages = 8;
 constexpr int kTcN = 256;                      // MMA N = tile columns
 constexpr uint64_t kTcWaitLimitNs = 2000000000ull;  // 2 s per wait
+static_assert(kTcStages == 2 && kTcParamSlots == 64 && kTcBStages == 8, "the roles' slot / stage / parity arithmetic");
 
 struct TcPlan {
   int n = 0, nt = 0, gl = 0;
@@ -256,7 +258,7 @@ struct TcSlot {
 };
 
 struct TcSmemLayout {
-  uint32_t a_off, b_off, bar_off, slot_off, eu_off, misc_off, lo_off, w_off, total;
+  uint32_t a_off, b_off, bar_off, slot_off, eu_off, ey_off, rs_off, misc_off, lo_off, w_off, total;
 };
 
 __host__ __device__ inline TcSmemLayout tc_layout(int n) {
@@ -272,6 +274,10 @@ __host__ __device__ inline TcSmemLayout tc_layout(int n) {
   o += kTcParamSlots * sizeof(TcSlot);
   L.eu_off = o;
   o += kTcN * 4;
+  L.ey_off = o;
+  o += 128 * 4;  // E_Y(y) per row
+  L.rs_off = o;
+  o += kTcBStages * 128 * 4;  // R_t(y) per B stage and row, written with the stage
   L.misc_off = o;
   o += 64;
   L.lo_off = o;
@@ -298,6 +304,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   uint64_t* acc_empty = acc_full + kTcStages;
   TcSlot* slots = reinterpret_cast<TcSlot*>(tc_smem + L.slot_off);
   float* EU = reinterpret_cast<float*>(tc_smem + L.eu_off);
+  float* EY = reinterpret_cast<float*>(tc_smem + L.ey_off);
+  float* Rs = reinterpret_cast<float*>(tc_smem + L.rs_off);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + L.misc_off);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tc_smem + L.misc_off + 4);
   double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
       mbar_init(&p_full[s], 1);
-      mbar_init(&p_empty[s], 2);  // the tile's producer warp + the MMA thread (tile consumed)
+      mbar_init(&p_empty[s], 1);  // the tile's producer warp (the only reader of the slot)
     }
     for (int s = 0; s < kTcBStages; ++s) {
       mbar_init(&b_full[s], 1);
@@ -368,6 +376,18 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         if ((u >> j2) & 1) e += row[n - 1 - j2];
     }
     EU[u] = (float)e;
+  }
+  // E_Y(y)
+  for (int y = tid; y < 128; y += kTcThreads) {
+    double e = 0.0;
+    for (int i = 0; i < 7; ++i) {
+      if (!((y >> i) & 1)) continue;
+      const double* row = Ws + (n - 9 - i) * n;
+      e += row[n - 9 - i];
+      for (int i2 = 0; i2 < i; ++i2)
+        if ((y >> i2) & 1) e += row[n - 9 - i2];
+    }
+    EY[y] = (float)e;
   }
   // t_lo tables: LO[p*16 + j] = (p^T W_TlU)_j (j < 8), LO[p*16 + 8 + i] = (p^T W_TlY)_i
   // (i < 7), LO[p*16 + 15] = energy of the t_lo bits p
@@ -467,42 +487,41 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     // ---------------------------------------------------------- MMA issue
     if (lane == 0) {
       const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
-      uint64_t issued = 0;
-      for (uint64_t j = 0; j < ntiles && ok; ++j) {
-        const int bs = (int)(j % kTcBStages);
-        const int as = (int)(j % kTcStages);
-        ok = mbar_wait(&b_full[bs], (uint32_t)((j / kTcBStages) & 1), abort_flag) &&
-             mbar_wait(&acc_empty[as], (uint32_t)(((j / kTcStages) & 1) ^ 1), abort_flag);
+      const uint32_t nt32 = (uint32_t)ntiles;
+      uint32_t issued = 0;
+      for (uint32_t j = 0; j < nt32 && ok; ++j) {
+        const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
+        const uint32_t as = j & 1u;
+        ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag) &&
+             mbar_wait(&acc_empty[as], ((j >> 1) & 1u) ^ 1u, abort_flag);
         if (!ok) break;
         tc_fence_after();
-        if (j >= (uint64_t)kTcStages) {
-          // every epilogue warp has released tile j-2 (it read that tile's parameters before
-          // its release, and MMA j-2 completed before the tile could be read): its B stage and
-          // parameter slot are free
-          const uint64_t jp = j - kTcStages;
-          mbar_arrive(&b_empty[jp % kTcBStages]);
-          mbar_arrive(&p_empty[jp % kTcParamSlots]);
-        }
+        // every epilogue warp has released tile j-2 (it read that tile's row terms before its
+        // release, and MMA j-2 completed before the tile could be read): its B stage is free
+        if (j >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(j - kTcStages) & (uint32_t)(kTcBStages - 1)]);
         const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
-        tc_mma(tmem + (uint32_t)as * (uint32_t)kTcN, adesc, bdesc);
+        tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc);
         tc_commit(&acc_full[as]);  // one commit per MMA
         issued = j + 1;
       }
       if (issued) {  // let the last MMA finish before the CTA can release TMEM
-        const uint64_t j = issued - 1;
-        mbar_wait(&acc_full[j % kTcStages], (uint32_t)((j / kTcStages) & 1), abort_flag);
+        const uint32_t j = issued - 1;
+        mbar_wait(&acc_full[j & 1u], (j >> 1) & 1u, abort_flag);
       }
     }
     __syncwarp();
   } else if (warp < 4) {
     // ---------------------------------------------------------- B producers (C_t columns)
     // warp 2 + (j & 1) fills tile j: rows u = lane + 32 r, r < 8 (u bits 5..7 = r)
-    for (uint64_t j = (uint64_t)(warp - 2); j < ntiles && ok; j += 2) {
-      const int s = (int)(j % kTcParamSlots);
-      const int bs = (int)(j % kTcBStages);
-      ok = mbar_wait(&p_full[s], (uint32_t)((j / kTcParamSlots) & 1), abort_flag);
+    // and the row terms R_t(y) = E_T(t) + E_Y(y) + (t^T W_TY) y of rows y = lane + 32 r, r < 4
+    const uint32_t nt32 = (uint32_t)ntiles;
+    for (uint32_t j = (uint32_t)(warp - 2); j < nt32 && ok; j += 2) {
+      const uint32_t s = j & (uint32_t)(kTcParamSlots - 1);
+      const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
+      ok = mbar_wait(&p_full[s], (j >> 6) & 1u, abort_flag);
       if (!ok) break;
       __half2 dg[8];
+      float rr[4];
       {
         const TcSlot& sl = slots[s];
         float s5 = 0.f;
@@ -518,12 +537,25 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
           if (r & 4) cr += f7;
           dg[r] = digits(EU[lane + 32 * r] + cr, P.exact);
         }
+        float g5 = sl.et;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+          if ((lane >> i) & 1) g5 += sl.g[i];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          float v = g5;
+          if (r & 1) v += sl.g[5];
+          if (r & 2) v += sl.g[6];
+          rr[r] = v + EY[lane + 32 * r];
+        }
       }
-      ok = mbar_wait(&b_empty[bs], (uint32_t)(((j / kTcBStages) & 1) ^ 1), abort_flag);
+      ok = mbar_wait(&b_empty[bs], ((j >> 3) & 1u) ^ 1u, abort_flag);
       if (!ok) break;
       unsigned char* Bst = Bsm + bs * kTcN * 32;
 #pragma unroll
       for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) Rs[bs * 128 + lane + 32 * r] = rr[r];
       fence_proxy_async();
       __syncwarp();
       if (lane == 0) {
@@ -536,39 +568,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     const int q = warp & 3;           // TMEM lane quarter (warp id % 4)
     const int cq = (warp - 4) >> 2;   // column quarter: columns 64*cq .. 64*cq+63
     const int y = q * 32 + lane;
-    float ybit[7];
-#pragma unroll
-    for (int i = 0; i < 7; ++i) ybit[i] = (float)((y >> i) & 1);
-    float ey;  // E_Y(y)
-    {
-      double e = 0.0;
-      for (int i = 0; i < 7; ++i) {
-        if (!((y >> i) & 1)) continue;
-        const double* row = Ws + (n - 9 - i) * n;
-        e += row[n - 9 - i];
-        for (int i2 = 0; i2 < i; ++i2)
-          if ((y >> i2) & 1) e += row[n - 9 - i2];
-      }
-      ey = (float)e;
-    }
     const float inv = P.inv_scale;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
-    const uint64_t gmask = (1ull << P.gl) - 1ull;
     const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)cq * 64u;
-    for (uint64_t j = 0; j < ntiles && ok; ++j) {
-      const int s = (int)(j % kTcParamSlots);
-      const int as = (int)(j % kTcStages);
-      ok = mbar_wait(&p_full[s], (uint32_t)((j / kTcParamSlots) & 1), abort_flag);
+    // 32-bit loop state (a CTA walks fewer than 2^32 tiles); records every 2^gl tiles,
+    // counted down from the CTA's first block (aligned to 2^gl)
+    const uint32_t nt32 = (uint32_t)ntiles;
+    uint32_t rec_left = 1u << P.gl;
+    uint64_t Jrec = (i_begin - P.tile_begin) >> P.gl;
+    for (uint32_t j = 0; j < nt32 && ok; ++j) {
+      const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
+      const uint32_t as = j & 1u;
+      // the B stage of tile j is full: its row terms are written (b_full cannot move on to
+      // tile j + 8 before this warp has released tile j)
+      ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag);
       if (!ok) break;
-      float R;
-      {
-        const TcSlot& sl = slots[s];
-        R = sl.et + ey;
-#pragma unroll
-        for (int i = 0; i < 7; ++i) R = fmaf(ybit[i], sl.g[i], R);
-      }
-      ok = mbar_wait(&acc_full[as], (uint32_t)((j / kTcStages) & 1), abort_flag);
+      const float R = Rs[bs * 128 + y];
+      ok = mbar_wait(&acc_full[as], (j >> 1) & 1u, abort_flag);
       if (!ok) break;
       tc_fence_after();
       const uint32_t ta = tbase + (uint32_t)as * (uint32_t)kTcN;
@@ -583,13 +600,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       if (lane == 0) mbar_arrive(&acc_empty[as]);  // the stage is free once the data is in registers
       const float m = fminf(min32(ra), min32(rb));
       rmin = fminf(rmin, m + R);
-      const uint64_t i = i_begin + j;
-      if ((i & gmask) == gmask) {
+      if (--rec_left == 0) {
         const float wm = warp_min_f(rmin);
-        if (lane == 0) {
-          const uint64_t J = (i >> P.gl) - (P.tile_begin >> P.gl);
-          P.rec[(J << 4) | ((uint64_t)cq << 2) | (uint64_t)q] = wm * inv;
-        }
+        if (lane == 0) P.rec[(Jrec << 4) | ((uint64_t)cq << 2) | (uint64_t)q] = wm * inv;
+        ++Jrec;
+        rec_left = 1u << P.gl;
         rmin = inf;
       }
     }
@@ -630,6 +645,7 @@ inline int tc_launch(const TcPlan& p, float* rec, void* scratch, cudaStream_t st
   uint64_t ctas = std::min<uint64_t>((uint64_t)sms, groups);
   uint64_t gpc = (groups + ctas - 1) / ctas;
   ctas = (groups + gpc - 1) / gpc;
+  if ((gpc << p.gl) >> 32) return 1;  // a CTA's tile count must fit 32 bits (n <= 54 on 148 SMs)
   TcParams P{};
   P.n = p.n;
   P.nt = p.nt;
