@@ -920,7 +920,63 @@ int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, dou
 
 int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
   if (!h || !form_out || n < 1 || n > qb::kMaxN || dtype_size(dtype) == 0) return QB_EINVAL;
-  *form_out = n >= 20 ? QB_FORM_GRAY : QB_FORM_EXACT;
+  if (n < 20) {  // the exact form is the only one below 20 variables
+    h->autotuned_form[n] = QB_FORM_EXACT;
+    *form_out = QB_FORM_EXACT;
+    return QB_OK;
+  }
+  // a seeded synthetic problem of the dtype's class: integer entries in [-100, 100] for
+  // integer dtypes (exact arithmetic), uniform [-1, 1) for float dtypes
+  const bool is_int = dtype >= QB_I8;
+  std::vector<double> Q((size_t)n * n);
+  uint64_t st = 0x9E3779B97F4A7C15ull ^ (uint64_t)n;
+  for (auto& v : Q) {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    v = is_int ? (double)((int64_t)(st % 201) - 100) : (double)(st >> 11) * 0x1.0p-52 - 1.0;
+  }
+  qb_problem p{};
+  p.n = n;
+  p.dtype = is_int ? QB_I64 : QB_F64;
+  std::vector<int64_t> Qi;
+  if (is_int) {
+    Qi.assign(Q.begin(), Q.end());
+    p.q = Qi.data();
+  } else {
+    p.q = Q.data();
+  }
+  p.ldq = n;
+  // time one shard of at most 2^36 states per form: pass 1 plus candidate re-evaluation
+  const int shard_bits = std::max(0, n - 36);
+  float best_ms = 0.f;
+  int best = QB_FORM_GRAY;
+  const int forms[2] = {QB_FORM_GRAY, QB_FORM_TC};
+  for (int f : forms) {
+    if (f == QB_FORM_TC && !qb::tc_supported(n)) continue;
+    qb_options o{};
+    o.form = f;
+    o.tie_rule = QB_TIE_QBF;
+    o.prefix_bits = -1;
+    o.shard_index = 0;
+    o.shard_count = 1 << shard_bits;
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {  // warm-up, then the timed call
+      double lmin = 0.0;
+      int rc = qb_solve_begin(h, &p, &o, &lmin);
+      if (rc) return rc;
+      qb_result r{};
+      rc = qb_solve_finish(h, lmin, &r);
+      if (rc) return rc;
+      ms = r.pass1_ms + r.pass2_ms;
+    }
+    if (best_ms == 0.f || ms < best_ms) {
+      best_ms = ms;
+      best = f;
+    }
+  }
+  h->autotuned_form[n] = best;
+  *form_out = best;
   return QB_OK;
 }
 

@@ -152,9 +152,11 @@ int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, cons
  * per prefix in update_global_minima (src/qubo_lib/solvers/qbf.py:395-412, 342-351). */
 int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, double* out);
 
-/* Pick the fastest form for problems of n variables and dtype by timing candidate kernel
- * configurations on the handle's device; the choice is cached in the handle and used by
- * QB_FORM_AUTO.  *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond
+/* Pick the fastest form for problems of n variables and dtype by timing the Gray-code and
+ * tensor-core forms (pass 1 + re-evaluation of one shard of at most 2^36 states) on a seeded
+ * synthetic problem of the dtype's class on the handle's device; the choice is cached in
+ * the handle (per n) and used by QB_FORM_AUTO.  n < 20 always gives QB_FORM_EXACT.
+ * *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond
  * QBF.define_chunk_size (src/qubo_lib/solvers/qbf.py:429-466), which picks a split. */
 int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out);
 
