@@ -18,6 +18,8 @@ QB_OK, QB_EINVAL, QB_ERANGE, QB_ENOMEM, QB_ECUDA, QB_ETIMEOUT, QB_ENODEV, QB_EOV
 QB_F32, QB_F64, QB_I8, QB_I16, QB_I32, QB_I64 = 1, 2, 3, 4, 5, 6
 FORMS = {"auto": 0, "gray": 1, "tc": 2, "exact": 3}
 FORM_NAMES = {v: k for k, v in FORMS.items()}
+FORM_NAMES[4] = "qb_f1_int16"
+QB_FLAG_INT16_WRAP = 1
 TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
 
 _DTYPES = {
@@ -143,10 +145,11 @@ class Handle:
 
     @staticmethod
     def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
-                max_candidates=0, stream=None) -> QbOptions:
+                max_candidates=0, stream=None, int16_wrap=False) -> QbOptions:
         return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
                          prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
-                         max_candidates=int(max_candidates), flags=0, stream=stream)
+                         max_candidates=int(max_candidates), flags=QB_FLAG_INT16_WRAP if int16_wrap else 0,
+                         stream=stream)
 
     def solve(self, Q: np.ndarray, **opts) -> dict:
         p, keep = self._problem(Q)

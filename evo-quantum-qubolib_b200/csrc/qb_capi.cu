@@ -15,6 +15,7 @@
 #include "qb_common.cuh"
 #include "qb_exact.cuh"
 #include "qb_gray.cuh"
+#include "qb_qbf1.cuh"
 #include "qb_reduce.cuh"
 #include "qb_tc.cuh"
 
@@ -627,8 +628,128 @@ int qb_solve_finish(qb_handle* h, double global_min, qb_result* r) {
   return QB_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// QB_F1 with the reference's int16 arithmetic (QB_FLAG_INT16_WRAP; qb_qbf1.cuh).
+int qbf1_wrap_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* r) {
+  memset(r, 0, sizeof(*r));
+  const int n = p->n;
+  if (p->dtype != QB_I16 || n < 19 || n > qb::kQbf1MaxN || o->fixed_bits != 0 || o->shard_count > 1 ||
+      p->ldq < n || !p->q)
+    return QB_EINVAL;
+  QB_CUDA(cudaSetDevice(h->device));
+  h->st = o->stream ? static_cast<cudaStream_t>(o->stream) : h->own;
+  h->pending = false;
+  h->kernels = 0;
+  h->h2d = h->d2h = 0;
+  // the int16 matrix, as int32
+  std::vector<int16_t> raw((size_t)n * n);
+  if (p->q_on_device) {
+    QB_CUDA(cudaMemcpy2DAsync(raw.data(), (size_t)n * 2, p->q, (size_t)p->ldq * 2, (size_t)n * 2, n,
+                              cudaMemcpyDeviceToHost, h->st));
+    QB_CUDA(cudaStreamSynchronize(h->st));
+    h->d2h += (int64_t)n * n * 2;
+  } else {
+    const int16_t* src = static_cast<const int16_t*>(p->q);
+    for (int i = 0; i < n; ++i) memcpy(raw.data() + (size_t)i * n, src + (size_t)i * p->ldq, (size_t)n * 2);
+  }
+  std::vector<int> Qi(raw.begin(), raw.end());
+  const int A = n - qb::kQbf1B;
+  const uint64_t steps = 1ull << A;
+  const size_t cols = (size_t)1 << qb::kQbf1B;
+  DevBuf* B = h->bat;
+  QB_CUDA(B[0].ensure(Qi.size() * sizeof(int)));
+  QB_CUDA(B[6].ensure(cols * sizeof(short)));
+  QB_CUDA(B[7].ensure((size_t)A * cols * sizeof(short)));
+  QB_CUDA(B[8].ensure(steps * sizeof(short)));
+  QB_CUDA(B[9].ensure((qb::kQbf1Threads + 1) * sizeof(unsigned long long)));
+  QB_CUDA(cudaMemcpyAsync(B[0].p, Qi.data(), Qi.size() * sizeof(int), cudaMemcpyHostToDevice, h->st));
+  h->h2d += (int64_t)(Qi.size() * sizeof(int));
+  const int* dQ = static_cast<const int*>(B[0].p);
+  short* BB = static_cast<short*>(B[6].p);
+  short* ABBA = static_cast<short*>(B[7].p);
+  short* AA = static_cast<short*>(B[8].p);
+  unsigned long long* key = static_cast<unsigned long long*>(B[9].p);
+  QB_CUDA(cudaMemsetAsync(key, 0xff, (qb::kQbf1Threads + 1) * sizeof(unsigned long long), h->st));
+  QB_CUDA(cudaEventRecord(h->ev[0], h->st));
+  qb::qbf1w_tables_kernel<<<(unsigned)(cols / 256), 256, (size_t)n * n * sizeof(int), h->st>>>(dQ, n, A, BB, ABBA);
+  qb::qbf1w_prefix_kernel<<<(unsigned)std::min<uint64_t>((steps + 255) / 256, (uint64_t)h->sm_count * 8), 256,
+                            (size_t)A * A * sizeof(int), h->st>>>(dQ, n, A, AA);
+  const uint64_t nchunks = std::min<uint64_t>(64, std::max<uint64_t>(4, steps));
+  const uint64_t chunk_len = (steps + nchunks - 1) / nchunks;
+  const size_t sm = (size_t)A * 1024 * sizeof(short);
+  QB_CUDA(cudaFuncSetAttribute(qb::qbf1w_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  QB_CUDA(cudaEventRecord(h->ev[4], h->st));
+  qb::qbf1w_search_kernel<<<dim3(qb::kQbf1Threads / 64, (unsigned)(nchunks / 4)), 256, sm, h->st>>>(
+      A, BB, ABBA, AA, chunk_len, key);
+  QB_CUDA(cudaEventRecord(h->ev[5], h->st));
+  h->kernels += 3;
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(h->hout.ensure(qb::kQbf1Threads * sizeof(unsigned long long)));
+  QB_CUDA(cudaMemcpyAsync(h->hout.p, key, qb::kQbf1Threads * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          h->st));
+  h->d2h += (int64_t)qb::kQbf1Threads * 8;
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  // the host's argmin over the threads' best values: the lowest thread among equals
+  const unsigned long long* hk = static_cast<const unsigned long long*>(h->hout.p);
+  int tid = 0;
+  for (int i = 1; i < qb::kQbf1Threads; ++i)
+    if ((hk[i] >> 40) < (hk[tid] >> 40)) tid = i;
+  if (hk[tid] == ~0ull) return QB_ECUDA;
+  const int best16 = (int)(hk[tid] >> 40) - 32768;
+  const uint64_t step = hk[tid] & ((1ull << 40) - 1);
+  const uint64_t prefix = qb::gray64(step);
+  qb::qbf1w_row_kernel<<<(unsigned)(cols / 256), 256, 0, h->st>>>(A, BB, ABBA, prefix, key + qb::kQbf1Threads);
+  ++h->kernels;
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(cudaEventRecord(h->ev[1], h->st));
+  QB_CUDA(cudaMemcpyAsync(h->hmisc.p, key + qb::kQbf1Threads, 8, cudaMemcpyDeviceToHost, h->st));
+  h->d2h += 8;
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  const uint64_t sfx = *static_cast<const unsigned long long*>(h->hmisc.p) & 0xffffffffull;
+  const uint64_t X = (prefix << qb::kQbf1B) | sfx;
+  double e = 0.0;  // exact energy of the reported state
+  for (int i = 0; i < n; ++i) {
+    if (!((X >> (n - 1 - i)) & 1)) continue;
+    for (int j = 0; j < n; ++j)
+      if ((X >> (n - 1 - j)) & 1) e += Qi[(size_t)i * n + j];
+  }
+  float p1 = 0.f, km = 0.f;
+  QB_CUDA(cudaEventElapsedTime(&p1, h->ev[0], h->ev[1]));
+  QB_CUDA(cudaEventElapsedTime(&km, h->ev[4], h->ev[5]));
+  r->best_x = X;
+  r->best_e = e;
+  r->best_e_int = best16;  // the value the reference reports (its int16 running sum)
+  r->order_key = ((uint64_t)tid << 40) | step;
+  r->pass1_min = (double)best16;
+  r->states = (int64_t)1 << n;
+  r->form_used = QB_FORM_QBF1_INT16;
+  r->is_integer = 1;
+  r->found = 1;
+  r->status = QB_OK;
+  r->pass1_ms = p1;
+  r->kernels = h->kernels;
+  r->kernel_ms = km;
+  r->h2d_bytes = h->h2d;
+  r->d2h_bytes = h->d2h;
+  return QB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* r) {
   if (!r) return QB_EINVAL;
+  if (h && p && o && (o->flags & QB_FLAG_INT16_WRAP)) {
+    if (o->tie_rule != QB_TIE_QB_F1) return QB_EINVAL;
+    QB_CUDA(h->hmisc.ensure(64));
+    const int rc = qbf1_wrap_solve(h, p, o, r);
+    if (rc) r->status = rc;
+    return rc;
+  }
   double lmin = 0.0;
   int rc = qb_solve_begin(h, p, o, &lmin);
   if (rc) {

@@ -15,7 +15,9 @@ Signatures, kwargs, errors and the returned Solution follow the reference:
             answer chosen with QB_F1's kernel order (lowest of its 16,384 threads, then the
             earliest Gray prefix, then the smallest suffix).  Energies are exact: where the
             reference's int16 arithmetic could wrap, ``solution.search['int16_wrap_possible']``
-            is set.
+            is set.  ``int16_wrap=True`` instead reproduces the reference's int16 arithmetic
+            (state and reported best_E as the reference gives them, even where its sums
+            overflow), for 19 <= N <= 46.
 * Parallel -- src/qubo_lib/solvers/parallel.py:20-158: bit fixing over splits_cnt = 2^k
             tasks.  On one device the split is a tie-rule detail of a single GPU search
             (tasks are prefix tiles inside the kernel); with several devices one worker
@@ -224,8 +226,9 @@ class QB_F1(SolverABC):
             raise ValueError(f"QB_F1 needs N >= 19 (B is fixed to 18), got N={self.N}")
         self.Q = Q
         self.timer.pick_time("build_Q")
+        wrap = bool(kwargs.get("int16_wrap", False))
         res = _lib.handle(dev).solve(Q, form=kwargs.get("form", "auto"), tie_rule="qb_f1", fixed_bits=0,
-                                     stream=stream)
+                                     stream=stream, int16_wrap=wrap)
         self.timer.pick_time("Kernel run time")
         best_X = res["best_X"]
         sol = Solution(self.N, 1, 1, problem.to_json(), self.json_str)
@@ -243,7 +246,10 @@ class QB_F1(SolverABC):
         sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_ms", "pass2_ms", "kernel_ms",
                                           "kernels", "h2d_bytes", "d2h_bytes")}
         sol.search["int16_wrap_possible"] = _int16_wrap_possible(Q)
-        if sol.search["int16_wrap_possible"]:
+        sol.search["int16_wrap"] = wrap
+        if wrap:  # the reference's answer: its int16 running value and the state it picks
+            sol.search["exact_E"] = float(res["best_E"])
+        elif sol.search["int16_wrap_possible"]:
             logger.warning("QB_F1: partial sums of Q exceed int16; the reference's int16 arithmetic could wrap, "
                            "this result is the exact minimum")
         return sol
@@ -333,6 +339,8 @@ class Parallel(SolverABC):
                 raise TypeError("Q dtype only np.int16 supported yet")
             if m < 19:
                 raise ValueError(f"QB_F1 needs N - log2(splits_cnt) >= 19, got {m}")
+            if kwargs.get("int16_wrap", False):
+                return self._solve_qbf1_int16(problem, Q, k, json_str, t0, kwargs)
             opts = dict(form=kwargs.get("form", "auto"), tie_rule="qb_f1", fixed_bits=k)
         devs = sorted(set(_parse_cuda(d) for d in self._devices))
         if len(devs) == 1:
@@ -373,6 +381,41 @@ class Parallel(SolverABC):
                                         time_to_solve_ms=r["time_ms"], states=r["states"]))
         sol.search = {k2: best[k2] for k2 in ("form", "candidate_records", "pass1_ms", "pass2_ms", "order_key")}
         sol.search["states"] = sum(r["states"] for r in results)
+        return sol
+
+    def _solve_qbf1_int16(self, problem, Q, k, json_str, t0, kwargs) -> Solution:
+        """Parallel(QB_F1) with the reference's int16 arithmetic, task by task as the reference
+        runs it (parallel.py:145-157, 225-320): ReducedProblem in int16 (its prefix_E and
+        reduced Q wrap as in reduced_problem.py:31-46), QB_F1 on each, the best of
+        best_E + prefix_E with strict < in task order."""
+        from .problems import Just_Q, ReducedProblem
+        dev = _parse_cuda(self._devices[0])
+        base = Just_Q(Q)
+        best = None
+        logs = []
+        for task in range(self._splits_cnt):
+            prefix = np.array([(task >> (k - 1 - i)) & 1 for i in range(k)])
+            rp = ReducedProblem(base, prefix)
+            part = QB_F1().solve(rp, device=f"cuda:{dev}", int16_wrap=True)
+            adj = part.best_E + rp.prefix_E
+            if best is None or adj < best[0]:
+                best = (adj, task, part)
+            logs.append(dict(task_id=task, worker_id=0, device=f"cuda:{dev}", time_to_solve_ms=part.time_to_solve_ms))
+        adj, task, part = best
+        N = problem.N
+        sol = Solution(N=N, epochs_cnt=self._splits_cnt, samples_cnt=1, problem_instance_json=problem.to_json(),
+                       solver_params_json=json_str)
+        sol.ising_offset = None
+        sol.solver_class = "QB_F1"
+        sol.best_E = adj
+        sol.energies = np.array([adj])
+        prefix = np.array([(task >> (k - 1 - i)) & 1 for i in range(k)], dtype=part.best_X.dtype)
+        sol.best_X = np.hstack([prefix, part.best_X])
+        sol.state_vectors = StateVectors(wide_vector_matrix=sol.best_X.reshape(1, -1))
+        sol.metrics = [{}]
+        sol.time_to_solve_ms = (time.perf_counter() - t0) * 1000
+        sol.worker_logs = logs
+        sol.search = dict(part.search, task=task)
         return sol
 
     @staticmethod

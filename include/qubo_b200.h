@@ -59,6 +59,14 @@ extern "C" {
 #define QB_FORM_GRAY 1   /* plain Gray-code SIMT kernel (fp32 or int32 arithmetic) */
 #define QB_FORM_TC 2     /* tcgen05 contraction form (f16 digits, fp32 accumulate) */
 #define QB_FORM_EXACT 3  /* FP64 / integer-exact enumeration (small n) */
+#define QB_FORM_QBF1_INT16 4  /* (reported only) QB_F1 in the reference's int16 arithmetic */
+
+/* qb_options.flags */
+#define QB_FLAG_INT16_WRAP 1  /* QB_TIE_QB_F1, int16 Q, 19 <= n <= 46: reproduce the reference
+                                 QB_F1's int16 arithmetic (its tables and running sums wrap
+                                 modulo 2^16), so that the state and the reported best_e_int
+                                 are the reference's even where its sums overflow; best_e is
+                                 the exact energy of that state (qbf1.py:86-133, 179-289) */
 
 /* tie rules */
 #define QB_TIE_QBF 0
@@ -84,7 +92,7 @@ typedef struct qb_options {
   int32_t shard_index;  /* multi-GPU: this rank's share of the search space ... */
   int32_t shard_count;  /* ... out of shard_count equal shares (1 = everything) */
   int32_t max_candidates; /* cap on candidate records re-scored per pass-2 launch (0 = default) */
-  int32_t flags;        /* reserved, 0 */
+  int32_t flags;        /* QB_FLAG_*, 0 = none */
   void* stream;         /* cudaStream_t to run on; NULL = the handle's own stream */
 } qb_options;
 

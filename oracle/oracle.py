@@ -255,3 +255,59 @@ def parallel_energy_arr_numpy(Q, k: int, A_sub: int) -> np.ndarray:
     per = E.reshape(1 << k, 1 << A_sub, 1 << B).min(axis=2)
     i = np.arange(1 << A_sub)
     return per[:, i ^ (i >> 1)].reshape(-1)
+
+
+def qbf1_int16_numpy(Q) -> dict:
+    """The reference QB_F1 restated with its int16 arithmetic (numpy int16 wraps modulo 2^16
+    as the reference's cupy int16 arrays and int16 kernel variables do):
+      prepare (src/qubo_lib/solvers/qbf1.py:86-133): B = 18, A = n - 18; BB = int16 suffix
+      energies; AA[i] = int16 E_pre(gray(i)); ABBA = (Q_0B + Q_1A^T) X_B^T in int16;
+      QB_F1_kernel (:179-249): 256 x 64 threads, thread tid owns columns
+      (tid >> 6) * 1024 + 64 * c + (tid & 63), c < 16; running int16 sums updated by the
+      flipped prefix row per Gray step; tested = int16(AA[i] + min); strict < keeps the
+      earliest step; the initial best is the min over the columns at prefix 0;
+      pack_results (:253-289): lowest thread with the smallest int16 best; its prefix's
+      int16 row argmin (first) gives the suffix; best_E is the thread's int16 value.
+    n in [19, 26] (vectorised over the 16384 threads)."""
+    Q = np.asarray(Q)
+    assert Q.dtype == np.int16
+    n = Q.shape[0]
+    A, B = n - 18, 18
+    S = np.arange(1 << B, dtype=np.int64)
+    XB = ((S[:, None] >> np.arange(B - 1, -1, -1)) & 1).astype(np.int64)       # 2^18 x 18
+    Q64 = Q.astype(np.int64)
+    BB = np.einsum("sj,jl,sl->s", XB, Q64[A:, A:], XB).astype(np.int16)
+    C = (Q[:A, A:] + Q[A:, :A].T).astype(np.int16).astype(np.int64)            # int16 sum, wraps
+    ABBA = (C @ XB.T).astype(np.int16)                                          # A x 2^18
+    I = np.arange(1 << A, dtype=np.int64)
+    G = I ^ (I >> 1)
+    XA = ((G[:, None] >> np.arange(A - 1, -1, -1)) & 1).astype(np.int64)
+    AA = np.einsum("ik,kl,il->i", XA, Q64[:A, :A], XA).astype(np.int16)
+    tid = np.arange(16384)
+    cols = ((tid >> 6) * 1024)[:, None] + 64 * np.arange(16)[None, :] + (tid & 63)[:, None]
+    E = BB[cols]                                                                # int16
+    best = E.min(axis=1)
+    bx = np.zeros(16384, dtype=np.int64)
+    for i in range(1, 1 << A):
+        g = i ^ (i >> 1)
+        prev = (i - 1) ^ ((i - 1) >> 1)
+        kb = (i & -i).bit_length() - 1
+        row = A - 1 - kb
+        if g > prev:
+            E = E + ABBA[row][cols]
+        else:
+            E = E - ABBA[row][cols]
+        m = E.min(axis=1)
+        t = (AA[i] + m).astype(np.int16)
+        upd = t < best
+        bx = np.where(upd, g, bx)
+        best = np.minimum(best, t)
+    idx = int(np.argmin(best))
+    p = int(bx[idx])
+    tmp = BB.copy()
+    for k in range(A):
+        if (p >> (A - 1 - k)) & 1:
+            tmp = tmp + ABBA[k]
+    s = int(np.argmin(tmp))
+    X = (p << B) | s
+    return {"best_E": int(best[idx]), "best_X_int": X, "exact_E": energy(Q, X)}

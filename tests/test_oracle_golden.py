@@ -149,3 +149,14 @@ def test_maxcut_test_instance_known_answer():
         Q[j, j] -= w
         Q[i, j] += 2 * w
     assert oracle.qbf_port(Q)["best_E"] == -19 == load_golden("maxcut_test.json")["qbf_best_E"]
+
+
+def test_qbf1_int16_restatement_equals_exact_rule_without_overflow():
+    """Where no int16 sum overflows, the int16 restatement of the reference QB_F1 gives the
+    same state and energy as the exact-energy QB_F1 order (pinned by the notebook's n=44
+    QB_F1 result on the GPU)."""
+    rng = np.random.default_rng(12)
+    for n in (19, 20):
+        Q = rng.integers(-60, 61, (n, n)).astype(np.int16)
+        a, b = oracle.qbf1_int16_numpy(Q), oracle.qbf1_numpy(Q)
+        assert (a["best_X_int"], a["best_E"]) == (b["best_X_int"], b["best_E"])
