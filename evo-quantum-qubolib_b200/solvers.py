@@ -419,19 +419,40 @@ class Parallel(SolverABC):
         return sol
 
     @staticmethod
-    def _run_workers(devs, Q, opts, timeout):
+    def _run_workers(devs, Q, opts, timeout, worker=None):
+        """One spawned process per device (worker, default _worker_main) searches a contiguous
+        share; the parent exchanges the pass-1 minima and collects the shares' results.  A
+        worker that reports an exception or exits without reporting raises RuntimeError; no
+        answer within ``timeout`` seconds (default 24 h, as the reference's scheduler) raises
+        TimeoutError.  Unlike the reference's scheduler (scheduler.py:26-45), partial results
+        are never merged."""
         ctx = mp.get_context("spawn")
         outbox = ctx.Queue()
         inboxes = [ctx.Queue() for _ in devs]
-        procs = [ctx.Process(target=_worker_main, args=(d, Q, opts, i, len(devs), inboxes[i], outbox))
+        target = worker or _worker_main
+        procs = [ctx.Process(target=target, args=(d, Q, opts, i, len(devs), inboxes[i], outbox))
                  for i, d in enumerate(devs)]
         for p in procs:
             p.start()
         deadline = time.time() + (timeout if timeout is not None else 24 * 3600)
+
+        def receive(done: dict):
+            while True:
+                left = deadline - time.time()
+                if left <= 0:
+                    raise _queue.Empty
+                try:
+                    kind, idx, val = outbox.get(timeout=min(0.5, left))
+                    return kind, idx, val
+                except _queue.Empty:
+                    for i, p in enumerate(procs):
+                        if i not in done and not p.is_alive() and outbox.empty():
+                            raise RuntimeError(f"worker {i} exited (code {p.exitcode}) without a result")
+
         try:
             mins = {}
             while len(mins) < len(devs):
-                kind, idx, val = outbox.get(timeout=max(0.0, deadline - time.time()))
+                kind, idx, val = receive(mins)
                 if kind == "err":
                     raise RuntimeError(f"worker {idx}: {val}")
                 mins[idx] = val
@@ -440,7 +461,7 @@ class Parallel(SolverABC):
                 q.put(gmin)
             results = {}
             while len(results) < len(devs):
-                kind, idx, val = outbox.get(timeout=max(0.0, deadline - time.time()))
+                kind, idx, val = receive(results)
                 if kind == "err":
                     raise RuntimeError(f"worker {idx}: {val}")
                 results[idx] = val
