@@ -274,6 +274,7 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
   }
   // tensor-core form
   qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc);
+  P.tc.stall = (o->flags & QB_FLAG_TEST_STALL) != 0;
   P.geom.kind = qb::kGeomTC;
   P.geom.gl = P.tc.gl;
   P.rec_begin = P.tc.rec_begin;

@@ -72,10 +72,12 @@ struct TcPlan {
   double eps = 0.0;        // per-state error bound, unscaled units
   uint64_t tile_begin = 0, tile_end = 0;  // this shard's Gray tile indices
   uint64_t rec_begin = 0, rec_count = 0, states = 0;
+  bool stall = false;      // test hook: the tile walk publishes nothing (waits expire)
 };
 
 struct TcParams {
   int n, nt, gl;
+  int stall;
   int exact;
   float inv_scale;
   const double* W;          // scaled W, n*n
@@ -416,7 +418,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   const uint32_t tmem = *tmem_slot;
 
   bool ok = true;
-  if (warp == 0) {
+  if (warp == 0 && P.stall) {
+    // test hook (QB_FLAG_TEST_STALL): no tile parameters are published, so every other
+    // role's bounded wait runs out; the CTA drains and the host reports QB_ETIMEOUT
+  } else if (warp == 0) {
     // ---------------------------------------------------------- tile walk
     // Every lane keeps the t_hi state (fp64, lane-redundant): fh = t_hi^T W_ThU, gh =
     // t_hi^T W_ThY, eh = E(t_hi), c_k = coupling of t_lo bit k with t_hi; lane l also
@@ -658,6 +663,7 @@ inline int tc_launch(const TcPlan& p, float* rec, void* scratch, cudaStream_t st
   P.groups_per_cta = gpc;
   P.rec = rec;
   P.err = err;
+  P.stall = p.stall ? 1 : 0;
   const TcSmemLayout L = tc_layout(p.n);
   // at least 120 KB so that one CTA (and one 512-column TMEM allocation) runs per SM
   const size_t smem = std::max<size_t>(L.total, 120 * 1024) + 1024;

@@ -67,6 +67,10 @@ extern "C" {
                                  modulo 2^16), so that the state and the reported best_e_int
                                  are the reference's even where its sums overflow; best_e is
                                  the exact energy of that state (qbf1.py:86-133, 179-289) */
+#define QB_FLAG_TEST_STALL 2  /* tests only, QB_FORM_TC: the search kernel's tile walk
+                                 publishes nothing, so the kernel's bounded waits run out
+                                 (about 2 s); the call returns QB_ETIMEOUT and the handle
+                                 and CUDA context stay usable */
 
 /* tie rules */
 #define QB_TIE_QBF 0
