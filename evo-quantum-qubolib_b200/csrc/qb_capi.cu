@@ -307,7 +307,7 @@ int run_pass1(qb_handle* h, Plan& P) {
       uint64_t g = std::min<uint64_t>(maxg, P.rec_count - off);
       qb::exact_records_kernel<<<(unsigned)g, qb::kExactThreads, sm, h->st>>>(
           pd, P.rule, P.geom, nullptr, nullptr, (int64_t)(P.rec_begin + P.rec_count), (int64_t)(P.rec_begin + off),
-          static_cast<qb::ExactOut*>(h->exout.p) + off);
+          static_cast<qb::ExactOut*>(h->exout.p) + off, 0);
       ++h->kernels;
     }
     QB_CUDA(cudaEventRecord(h->ev[5], h->st));
@@ -504,20 +504,33 @@ int rescore(qb_handle* h, const Plan& P, const qb::TieRule& rule, const qb::RecG
   }
   if (maxf > qb::kExactMaxFree) return QB_EINVAL;
   const qb::ProblemDev pd{P.n, static_cast<const double*>(h->W.p)};
-  QB_CUDA(h->exout.ensure((size_t)count * sizeof(qb::ExactOut)));
+  // few candidate records: split each over several CTAs (at least 2^12 states per CTA)
+  int sb = 0;
+  while (sb < maxf - 12 && ((int64_t)count << (sb + 1)) <= 2 * (int64_t)h->sm_count) ++sb;
+  const size_t nout = (size_t)count << sb;
+  QB_CUDA(h->exout.ensure(nout * sizeof(qb::ExactOut)));
   size_t sm = qb::exact_smem_bytes(P.n, maxf);
   QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  qb::exact_records_kernel<<<count, qb::kExactThreads, sm, h->st>>>(pd, rule, geom,
-                                                                     static_cast<const uint64_t*>(h->cand.p), nullptr,
-                                                                     count, 0, static_cast<qb::ExactOut*>(h->exout.p));
+  qb::exact_records_kernel<<<(unsigned)nout, qb::kExactThreads, sm, h->st>>>(
+      pd, rule, geom, static_cast<const uint64_t*>(h->cand.p), nullptr, count, 0,
+      static_cast<qb::ExactOut*>(h->exout.p), sb);
   ++h->kernels;
   QB_CUDA(cudaGetLastError());
-  QB_CUDA(h->hout.ensure((size_t)count * sizeof(qb::ExactOut)));
-  QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, (size_t)count * sizeof(qb::ExactOut), cudaMemcpyDeviceToHost, h->st));
-  h->d2h += (int64_t)count * (int64_t)sizeof(qb::ExactOut);
+  QB_CUDA(h->hout.ensure(nout * sizeof(qb::ExactOut)));
+  QB_CUDA(cudaMemcpyAsync(h->hout.p, h->exout.p, nout * sizeof(qb::ExactOut), cudaMemcpyDeviceToHost, h->st));
+  h->d2h += (int64_t)(nout * sizeof(qb::ExactOut));
   QB_CUDA(cudaStreamSynchronize(h->st));
   const qb::ExactOut* eo = static_cast<const qb::ExactOut*>(h->hout.p);
-  out.assign(eo, eo + count);
+  // the lexicographic minimum over each record's parts
+  out.resize(count);
+  for (int c = 0; c < count; ++c) {
+    qb::ExactOut b = eo[(size_t)c << sb];
+    for (int q = 1; q < (1 << sb); ++q) {
+      const qb::ExactOut& o = eo[((size_t)c << sb) + q];
+      if (o.e < b.e || (o.e == b.e && o.key < b.key)) b = o;
+    }
+    out[c] = b;
+  }
   return QB_OK;
 }
 
@@ -1028,7 +1041,7 @@ int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, dou
   for (uint64_t off = 0; off < count; off += maxg) {
     const uint64_t g = std::min<uint64_t>(maxg, count - off);
     qb::exact_records_kernel<<<(unsigned)g, qb::kExactThreads, sm, h->st>>>(
-        pd, rule, geom, nullptr, nullptr, (int64_t)count, (int64_t)off, static_cast<qb::ExactOut*>(h->exout.p) + off);
+        pd, rule, geom, nullptr, nullptr, (int64_t)count, (int64_t)off, static_cast<qb::ExactOut*>(h->exout.p) + off, 0);
     ++h->kernels;
   }
   QB_CUDA(cudaGetLastError());
@@ -1308,7 +1321,7 @@ int noalloc_run(int device, const double* q_dev, int n, int is_integer, int pref
   const size_t sm2 = qb::exact_smem_bytes(n, maxf);
   QB_CUDA(cudaFuncSetAttribute(qb::exact_records_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   qb::exact_records_kernel<<<kNoAllocCands, qb::kExactThreads, sm2, st>>>(pd, rule, geom, cand, &misc->cand_count, 0, 0,
-                                                                         eo);
+                                                                         eo, 0);
   noalloc_final_kernel<<<1, 256, 0, st>>>(eo, misc, kNoAllocCands, is_integer ? 1 : 0, out_dev);
   QB_CUDA(cudaGetLastError());
   return QB_OK;

@@ -45,11 +45,13 @@ __device__ __forceinline__ bool lex_less(double e1, uint64_t k1, double e2, uint
   return e1 < e2 || (e1 == e2 && k1 < k2);
 }
 
-// One CTA (kExactThreads threads) evaluates record rid exactly and thread 0 writes the
-// record's lexicographic minimum to *out_slot.  smem_d: exact_smem_bytes(n, f) of dynamic
-// shared memory.
+// One CTA (kExactThreads threads) evaluates record rid exactly -- or, with split_bits > 0,
+// part `part` of it: the record's top split_bits free bits fixed to the bits of part (at
+// most f - 8 of them) -- and thread 0 writes the lexicographic minimum to *out_slot.
+// smem_d: exact_smem_bytes(n, f) of dynamic shared memory.
 __device__ __forceinline__ void exact_record_body(const ProblemDev& P, const TieRule& R, const RecGeom& G,
-                                                  uint64_t rid, ExactOut* __restrict__ out_slot, double* smem_d) {
+                                                  uint64_t rid, ExactOut* __restrict__ out_slot, double* smem_d,
+                                                  int part = 0, int split_bits = 0) {
   const int n = P.n;
   double* Ws = smem_d;                       // n*n
   double* Wl = Ws + n * n;                   // L*L couplings among low free variables
@@ -72,7 +74,10 @@ __device__ __forceinline__ void exact_record_body(const ProblemDev& P, const Tie
     nfree = c;
   }
   __syncthreads();
-  const int f = nfree;
+  const int sb = split_bits < nfree - 8 ? split_bits : (nfree > 8 ? nfree - 8 : 0);
+  const int f = nfree - sb;  // the top sb free bits are fixed by part
+  for (int j = 0; j < sb; ++j)
+    if ((part >> j) & 1) base |= 1ull << pos[f + j];
   const int tb = f < 8 ? f : 8;  // thread-selecting bits
   const int L = f - tb;          // bits walked per thread
   for (int i = threadIdx.x; i < L * L; i += blockDim.x) {
@@ -158,18 +163,22 @@ __device__ __forceinline__ void exact_record_body(const ProblemDev& P, const Tie
   }
 }
 
-// rec_ids: candidate record indices (nullptr: record = rec_offset + blockIdx.x).
+// rec_ids: candidate record indices (nullptr: record = rec_offset + block).
 // count_ptr: number of valid entries (nullptr: count_static).
+// split_bits: 2^split_bits CTAs per record (block = blockIdx.x >> split_bits); outputs are
+// indexed (slot << split_bits) | part.
 __global__ void __launch_bounds__(kExactThreads)
 exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restrict__ rec_ids,
                      const int* __restrict__ count_ptr, int64_t count_static, int64_t rec_offset,
-                     ExactOut* __restrict__ out) {
+                     ExactOut* __restrict__ out, int split_bits) {
   extern __shared__ double smem_d[];
-  const int64_t slot = (int64_t)blockIdx.x + (rec_ids ? rec_offset : 0);
+  const int64_t blk = (int64_t)(blockIdx.x >> split_bits);
+  const int part = (int)(blockIdx.x & ((1u << split_bits) - 1u));
+  const int64_t slot = blk + (rec_ids ? rec_offset : 0);
   const int64_t count = count_ptr ? (int64_t)(*count_ptr) : count_static;
   if (slot >= count) return;
-  const uint64_t rid = rec_ids ? rec_ids[slot] : (uint64_t)(rec_offset + blockIdx.x);
-  exact_record_body(P, R, G, rid, out + slot, smem_d);
+  const uint64_t rid = rec_ids ? rec_ids[slot] : (uint64_t)(rec_offset + blk);
+  exact_record_body(P, R, G, rid, out + ((slot << split_bits) | part), smem_d, part, split_bits);
 }
 
 inline size_t exact_smem_bytes(int n, int f) {
