@@ -104,14 +104,14 @@ __host__ __device__ __forceinline__ void record_states(const RecGeom& g, uint64_
     *base = (gray64(I) << (g.sbits + g.b)) | (cb << 13) | (w << 10);
     *freem = (mask64(g.sbits) << g.b) | mask64(10);
   } else if (g.kind == kGeomTC) {
-    // r = (block << 4) | (column quarter c << 2) | TMEM lane quarter q: the Gray tiles of
+    // r = (block << 3) | (column half h << 2) | TMEM lane quarter q: the Gray tiles of
     // block J (t >> gl = gray(J), low gl bits of t free), rows 32q..32q+31 (y's top 2
-    // bits = q), columns 64c..64c+63 (u's top 2 bits = c)
+    // bits = q), columns 128h..128h+127 (u's top bit = h)
     uint64_t q = r & 3ull;
-    uint64_t c = (r >> 2) & 3ull;
-    uint64_t J = r >> 4;
-    *base = (gray64(J) << (15 + g.gl)) | (q << 13) | (c << 6);
-    *freem = (mask64(g.gl) << 15) | (mask64(5) << 8) | mask64(6);
+    uint64_t h = (r >> 2) & 1ull;
+    uint64_t J = r >> 3;
+    *base = (gray64(J) << (15 + g.gl)) | (q << 13) | (h << 7);
+    *freem = (mask64(g.gl) << 15) | (mask64(5) << 8) | mask64(7);
   } else {
     *base = r << g.fbits;
     *freem = mask64(g.fbits);

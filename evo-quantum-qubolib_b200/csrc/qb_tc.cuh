@@ -32,9 +32,10 @@
 //   warp 1      TMEM allocation and MMA issue (one elected thread)
 //   warps 2-3   B producers, alternate tiles: C_t(u) digits into the B stage (generic
 //               stores + proxy fence) and the 128 row terms R_t(y) beside it
-//   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4)..+31 and the column quarter
-//               64*((w-4)/4)..+63 of every tile; it releases the accumulator stage as soon
-//               as its loads have landed, then reduces
+//   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4)..+31; warps 4-11 take the even
+//               tiles, 12-19 the odd ones, each a 128-column half in two rounds; a warp
+//               releases the accumulator stage as soon as its loads have landed, then
+//               reduces (so the 4 warps of a scheduler alternate between the two stages)
 // Pipelines on mbarriers: 64 tile-parameter slots (walk -> producers), 8 B stages
 // (producers -> MMA and epilogue), 2 accumulator stages.  One tcgen05.commit per MMA
 // (accumulator full); the MMA thread frees tile j-2's B stage when the epilogue's release
@@ -42,8 +43,8 @@
 // Every wait is bounded (%globaltimer): on timeout the waiting role raises an error flag,
 // the CTA drains and frees TMEM, and the host reports QB_ETIMEOUT.
 //
-// Records: every 2^gl tiles (gl >= 5) each epilogue warp writes the minimum over its 32
-// rows x 64 columns x 2^gl tiles.
+// Records: per block of 2^gl tiles (gl >= 5), 8 records of 32 rows x 128 columns x 2^gl
+// tiles, each the atomic minimum of the two warps (even and odd tiles) that cover it.
 //
 // Integer Q with sum|Q| <= 2^22 is exact (all partial sums stay below 2^24 in fp32).
 // Otherwise every value is within tc_error_bound() of the exact energy.
@@ -84,7 +85,7 @@ struct TcParams {
   uint64_t tile_begin;      // shard start (aligned to 2^gl)
   uint64_t groups;          // record blocks (2^gl tiles each) in this shard
   uint64_t groups_per_cta;  // contiguous blocks per CTA (last CTA may have fewer)
-  float* rec;               // rec[0] = record (tile_begin >> gl) << 4
+  float* rec;               // rec[0] = record (tile_begin >> gl) << 3
   unsigned* err;            // error word
 };
 
@@ -108,15 +109,15 @@ inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard
     p->scale = std::ldexp(1.0, e);
     p->eps = tc_error_bound(abs_sum);
   }
-  p->gl = std::max(5, p->nt - 18);  // runs of 32 tiles; at most 2^22 records (16 per block)
+  p->gl = std::max(5, p->nt - 18);  // runs of 32 tiles; at most 2^21 records (8 per block)
   uint64_t groups = 1ull << (p->nt - p->gl);
   unsigned __int128 g = groups;
   uint64_t gb = (uint64_t)(g * (unsigned)shard_idx / (unsigned)shard_cnt);
   uint64_t ge = (uint64_t)(g * (unsigned)(shard_idx + 1) / (unsigned)shard_cnt);
   p->tile_begin = gb << p->gl;
   p->tile_end = ge << p->gl;
-  p->rec_begin = gb << 4;
-  p->rec_count = (ge - gb) << 4;
+  p->rec_begin = gb << 3;
+  p->rec_count = (ge - gb) << 3;
   p->states = (p->tile_end - p->tile_begin) << 15;
 }
 
@@ -325,6 +326,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
 
   // ---------------------------------------------------------------- set-up
   for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
+  // this CTA's records start at +inf (the epilogue folds into them with atomic minima)
+  for (uint64_t r = (g0 << 3) + (uint64_t)tid; r < (g1 << 3); r += kTcThreads) P.rec[r] = __int_as_float(0x7f800000);
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
       mbar_init(&p_full[s], 1);
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     }
     for (int s = 0; s < kTcStages; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], kTcEpiWarps);
+      mbar_init(&acc_empty[s], kTcEpiWarps / 2);  // the 8 warps that read this stage
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -571,45 +574,62 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   } else {
     // ---------------------------------------------------------- epilogue
     const int q = warp & 3;           // TMEM lane quarter (warp id % 4)
-    const int cq = (warp - 4) >> 2;   // column quarter: columns 64*cq .. 64*cq+63
+    const int cq = (warp - 4) >> 2;   // 0..3: (tile parity, column half) below
     const int y = q * 32 + lane;
     const float inv = P.inv_scale;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
-    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)cq * 64u;
-    // 32-bit loop state (a CTA walks fewer than 2^32 tiles); records every 2^gl tiles,
-    // counted down from the CTA's first block (aligned to 2^gl)
+    // warps 4-11 take the even tiles (accumulator stage 0), warps 12-19 the odd ones (stage 1),
+    // so the four warps sharing a scheduler work on different tiles and one stage's waits
+    // overlap the other stage's minima; each reads 128 columns (column half hh) in two
+    // 64-column rounds and releases the stage once the second round has landed
+    const uint32_t sp = (uint32_t)cq >> 1;   // tile parity = accumulator stage
+    const uint32_t hh = (uint32_t)cq & 1u;   // column half
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+    // 32-bit loop state (a CTA walks fewer than 2^32 tiles); records every 2^gl tiles (2^(gl-1)
+    // of this warp's parity), counted down from the CTA's first block (aligned to 2^gl)
     const uint32_t nt32 = (uint32_t)ntiles;
-    uint32_t rec_left = 1u << P.gl;
+    uint32_t rec_left = 1u << (P.gl - 1);
     uint64_t Jrec = (i_begin - P.tile_begin) >> P.gl;
-    for (uint32_t j = 0; j < nt32 && ok; ++j) {
+    for (uint32_t j = sp; j < nt32 && ok; j += 2) {
       const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-      const uint32_t as = j & 1u;
       // the B stage of tile j is full: its row terms are written (b_full cannot move on to
       // tile j + 8 before this warp has released tile j)
       ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag);
       if (!ok) break;
       const float R = Rs[bs * 128 + y];
-      ok = mbar_wait(&acc_full[as], (j >> 1) & 1u, abort_flag);
+      ok = mbar_wait(&acc_full[sp], (j >> 1) & 1u, abort_flag);
       if (!ok) break;
       tc_fence_after();
-      const uint32_t ta = tbase + (uint32_t)as * (uint32_t)kTcN;
       uint32_t ra[32], rb[32];
-      QB_TC_LD32(ta, ra);
-      QB_TC_LD32(ta + 32, rb);
+      QB_TC_LD32(tbase, ra);
+      QB_TC_LD32(tbase + 32, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      const float m1 = fminf(min32(ra), min32(rb));
+      QB_TC_LD32(tbase + 64, ra);
+      QB_TC_LD32(tbase + 96, rb);
       tc_wait_ld();
       reg_fence32(ra);
       reg_fence32(rb);
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[as]);  // the stage is free once the data is in registers
-      const float m = fminf(min32(ra), min32(rb));
+      if (lane == 0) mbar_arrive(&acc_empty[sp]);  // the stage is free once the data is in registers
+      const float m = fminf(m1, fminf(min32(ra), min32(rb)));
       rmin = fminf(rmin, m + R);
       if (--rec_left == 0) {
-        const float wm = warp_min_f(rmin);
-        if (lane == 0) P.rec[(Jrec << 4) | ((uint64_t)cq << 2) | (uint64_t)q] = wm * inv;
+        // both parities' warps of (column half, lane quarter) fold into one record
+        const float wm = warp_min_f(rmin) * inv;
+        if (lane == 0) {
+          float* dst = P.rec + ((Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+          if (wm >= 0.f)
+            atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+          else
+            atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+        }
         ++Jrec;
-        rec_left = 1u << P.gl;
+        rec_left = 1u << (P.gl - 1);
         rmin = inf;
       }
     }
