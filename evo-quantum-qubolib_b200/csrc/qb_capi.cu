@@ -421,8 +421,12 @@ int qb_handle_destroy(qb_handle* h) {
   return QB_OK;
 }
 
-int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, double* local_min) {
-  if (!h || !p || !o || !local_min) return QB_EINVAL;
+}  // extern "C"
+
+namespace {
+
+// validation, problem upload and the pass-1 launch of qb_solve_begin
+int begin_launch(qb_handle* h, const qb_problem* p, const qb_options* o, Plan& P) {
   if (p->n < 1 || p->n > qb::kMaxN || !p->q || p->ldq < p->n || dtype_size(p->dtype) == 0) return QB_EINVAL;
   if (o->shard_count > 1 && (o->shard_index < 0 || o->shard_index >= o->shard_count)) return QB_EINVAL;
   QB_CUDA(cudaSetDevice(h->device));
@@ -431,7 +435,6 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
   h->kernels = 0;
   h->h2d = h->d2h = 0;
   h->cap = o->max_candidates > 0 ? o->max_candidates : kDefaultCap;
-  Plan P;
   P.n = p->n;
   std::vector<double> W;
   int rc = load_problem(h, p, W, &P.abs_sum, &P.is_int);
@@ -446,8 +449,11 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
   QB_CUDA(h->misc.ensure(64));
   QB_CUDA(h->hmisc.ensure(64));
   QB_CUDA(cudaEventRecord(h->ev[0], h->st));
-  rc = run_pass1(h, P);
-  if (rc) return rc;
+  return run_pass1(h, P);
+}
+
+// the rest of qb_solve_begin: the pass-1 minimum on the host
+int begin_finish_pass1(qb_handle* h, Plan& P, double* local_min) {
   double lmin = INFINITY;
   if (P.form == QB_FORM_EXACT) {
     QB_CUDA(cudaEventRecord(h->ev[1], h->st));
@@ -487,6 +493,104 @@ int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, doubl
   h->pending = true;
   *local_min = lmin;
   return QB_OK;
+}
+
+// qb_solve of one whole problem (Gray or tensor-core form, QB_TIE_QBF / QB_TIE_NATURAL):
+// minimum, threshold, selection, exact re-evaluation and the final pick all on the device,
+// then one copy of the answer to the host.  Returns -1 when the candidates overflow the cap
+// (the caller then takes the two-phase path with a larger cap).
+int solve_fused(qb_handle* h, const Plan& P, qb_result* r) {
+  char* m = static_cast<char*>(h->misc.p);  // [0] min key, [8] thr, [16] flag, [20] count, [24] best
+  uint32_t* mk = reinterpret_cast<uint32_t*>(m);
+  double* thr = reinterpret_cast<double*>(m + 8);
+  int* flag = reinterpret_cast<int*>(m + 16);
+  int* count = reinterpret_cast<int*>(m + 20);
+  qb::ExactOut* best = reinterpret_cast<qb::ExactOut*>(m + 24);
+  const unsigned* err = P.form == QB_FORM_TC ? static_cast<const unsigned*>(h->tcscratch.p) : nullptr;
+  QB_CUDA(cudaMemsetAsync(mk, 0xff, sizeof(uint32_t), h->st));
+  if (P.rec_count) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((P.rec_count + 255) / 256, (uint64_t)h->sm_count * 8);
+    qb::rec_min_kernel<<<blocks, 256, 0, h->st>>>(static_cast<const float*>(h->rec.p), (int64_t)P.rec_count, mk);
+    ++h->kernels;
+  }
+  QB_CUDA(cudaEventRecord(h->ev[1], h->st));
+  QB_CUDA(cudaEventRecord(h->ev[2], h->st));
+  qb::rec_threshold_kernel<<<1, 1, 0, h->st>>>(mk, P.eps, P.is_int ? 1 : 0, err, thr, flag, count);
+  QB_CUDA(h->cand.ensure((size_t)h->cap * sizeof(uint64_t)));
+  if (P.rec_count) {
+    const unsigned blocks = (unsigned)std::min<uint64_t>((P.rec_count + 255) / 256, (uint64_t)h->sm_count * 8);
+    qb::rec_select_dev_kernel<<<blocks, 256, 0, h->st>>>(static_cast<const float*>(h->rec.p), (int64_t)P.rec_count,
+                                                         (int64_t)P.rec_begin, thr, flag,
+                                                         static_cast<uint64_t*>(h->cand.p), count, h->cap);
+  }
+  int maxf = 0;
+  {
+    uint64_t b, f;
+    qb::record_states(P.geom, 0, &b, &f);
+    maxf = __builtin_popcountll(f & qb::mask64(P.n));
+  }
+  if (maxf > qb::kExactMaxFree) return QB_EINVAL;
+  const int sb = std::max(0, std::min(4, maxf - 12));
+  QB_CUDA(h->exout.ensure(((size_t)h->cap << sb) * sizeof(qb::ExactOut)));
+  const qb::ProblemDev pd{P.n, static_cast<const double*>(h->W.p)};
+  const size_t sm = qb::exact_smem_bytes(P.n, maxf);
+  QB_CUDA(cudaFuncSetAttribute(qb::exact_candidates_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  qb::exact_candidates_kernel<<<(unsigned)(2 * h->sm_count), qb::kExactThreads, sm, h->st>>>(
+      pd, P.rule, P.geom, static_cast<const uint64_t*>(h->cand.p), count, h->cap, sb,
+      static_cast<qb::ExactOut*>(h->exout.p));
+  qb::exact_final_kernel<<<1, 256, 0, h->st>>>(static_cast<const qb::ExactOut*>(h->exout.p), count, h->cap, sb, flag,
+                                               best);
+  h->kernels += 4;
+  QB_CUDA(cudaGetLastError());
+  QB_CUDA(cudaEventRecord(h->ev[3], h->st));
+  QB_CUDA(cudaMemcpyAsync(h->hmisc.p, m, 48, cudaMemcpyDeviceToHost, h->st));
+  h->d2h += 48;
+  unsigned herr = 0;
+  if (err) {
+    QB_CUDA(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, h->st));
+    h->d2h += (int64_t)sizeof(unsigned);
+  }
+  QB_CUDA(cudaStreamSynchronize(h->st));
+  if (herr & qb::kErrTimeout) return QB_ETIMEOUT;
+  const char* hm = static_cast<const char*>(h->hmisc.p);
+  const uint32_t key = *reinterpret_cast<const uint32_t*>(hm);
+  const int zero = *reinterpret_cast<const int*>(hm + 16);
+  const int cnt = *reinterpret_cast<const int*>(hm + 20);
+  if (!zero && cnt > h->cap) return -1;
+  const qb::ExactOut b = *reinterpret_cast<const qb::ExactOut*>(hm + 24);
+  const bool found = zero ? (P.rec_begin == 0 && P.rec_count > 0) : cnt > 0;
+  memset(r, 0, sizeof(*r));
+  r->form_used = P.form;
+  r->is_integer = P.is_int ? 1 : 0;
+  r->pass1_min = (P.rec_count && key != 0xffffffffu) ? (double)qb::key2f(key) : INFINITY;
+  r->err_bound = P.eps;
+  r->states = (int64_t)P.states;
+  r->candidate_records = zero ? 0 : cnt;
+  QB_CUDA(cudaEventElapsedTime(&r->pass1_ms, h->ev[0], h->ev[1]));
+  QB_CUDA(cudaEventElapsedTime(&r->pass2_ms, h->ev[2], h->ev[3]));
+  QB_CUDA(cudaEventElapsedTime(&r->kernel_ms, h->ev[4], h->ev[5]));
+  r->found = found ? 1 : 0;
+  r->best_x = b.x;
+  r->best_e = found ? b.e : INFINITY;
+  r->best_e_int = (found && P.is_int) ? (int64_t)llround(b.e) : 0;
+  r->order_key = b.key;
+  r->kernels = h->kernels;
+  r->h2d_bytes = h->h2d;
+  r->d2h_bytes = h->d2h;
+  r->status = QB_OK;
+  return QB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qb_solve_begin(qb_handle* h, const qb_problem* p, const qb_options* o, double* local_min) {
+  if (!h || !p || !o || !local_min) return QB_EINVAL;
+  Plan P;
+  int rc = begin_launch(h, p, o, P);
+  if (rc) return rc;
+  return begin_finish_pass1(h, P, local_min);
 }
 
 namespace {
@@ -764,8 +868,31 @@ int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* 
     if (rc) r->status = rc;
     return rc;
   }
+  if (!h || !p || !o) {
+    memset(r, 0, sizeof(*r));
+    r->status = QB_EINVAL;
+    return QB_EINVAL;
+  }
+  Plan P;
+  int rc = begin_launch(h, p, o, P);
+  if (rc) {
+    memset(r, 0, sizeof(*r));
+    r->status = rc;
+    return rc;
+  }
+  if (o->shard_count <= 1 && P.form != QB_FORM_EXACT && P.rule.kind != qb::kTieQBF1) {
+    rc = solve_fused(h, P, r);
+    if (rc >= 0) {
+      if (rc) {
+        memset(r, 0, sizeof(*r));
+        r->status = rc;
+      }
+      return rc;
+    }
+    // too many candidate records for the cap: the two-phase path grows it
+  }
   double lmin = 0.0;
-  int rc = qb_solve_begin(h, p, o, &lmin);
+  rc = begin_finish_pass1(h, P, &lmin);
   if (rc) {
     memset(r, 0, sizeof(*r));
     r->status = rc;

@@ -181,6 +181,65 @@ exact_records_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restr
   exact_record_body(P, R, G, rid, out + ((slot << split_bits) | part), smem_d, part, split_bits);
 }
 
+// The candidate records listed in rec_ids[0 .. min(*count_ptr, cap)), each split into
+// 2^split_bits parts, as a grid-stride loop over (record, part) items: the host launches it
+// before it knows the count.  Outputs at (slot << split_bits) | part.
+__global__ void __launch_bounds__(kExactThreads)
+exact_candidates_kernel(ProblemDev P, TieRule R, RecGeom G, const uint64_t* __restrict__ rec_ids,
+                        const int* __restrict__ count_ptr, int cap, int split_bits, ExactOut* __restrict__ out) {
+  extern __shared__ double smem_d[];
+  const int count = min(*count_ptr, cap);
+  const int64_t items = (int64_t)count << split_bits;
+  for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
+    __syncthreads();  // the previous item's shared-memory readers are done
+    const int64_t slot = w >> split_bits;
+    const int part = (int)(w & ((1 << split_bits) - 1));
+    exact_record_body(P, R, G, rec_ids[slot], out + w, smem_d, part, split_bits);
+  }
+}
+
+// One CTA: the lexicographic minimum of the first min(*count_ptr, cap) << split_bits
+// outputs into *best (x = 0 with energy 0 and key 0 when *zero_flag is set).
+__global__ void exact_final_kernel(const ExactOut* __restrict__ out, const int* __restrict__ count_ptr, int cap,
+                                   int split_bits, const int* __restrict__ zero_flag, ExactOut* __restrict__ best) {
+  __shared__ double se[32];
+  __shared__ uint64_t sk[32], sx[32];
+  const int64_t items = (int64_t)min(*count_ptr, cap) << split_bits;
+  double be = __longlong_as_double(0x7ff0000000000000ll);
+  uint64_t bk = ~0ull, bx = 0;
+  for (int64_t i = threadIdx.x; i < items; i += blockDim.x)
+    if (lex_less(out[i].e, out[i].key, be, bk)) {
+      be = out[i].e;
+      bk = out[i].key;
+      bx = out[i].x;
+    }
+  for (int off = 16; off; off >>= 1) {
+    const double oe = __shfl_down_sync(0xffffffffu, be, off);
+    const uint64_t ok = __shfl_down_sync(0xffffffffu, bk, off);
+    const uint64_t ox = __shfl_down_sync(0xffffffffu, bx, off);
+    if (lex_less(oe, ok, be, bk)) {
+      be = oe;
+      bk = ok;
+      bx = ox;
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    se[threadIdx.x >> 5] = be;
+    sk[threadIdx.x >> 5] = bk;
+    sx[threadIdx.x >> 5] = bx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (lex_less(se[w], sk[w], be, bk)) {
+        be = se[w];
+        bk = sk[w];
+        bx = sx[w];
+      }
+    *best = *zero_flag ? ExactOut{0.0, 0ull, 0ull} : ExactOut{be, bk, bx};
+  }
+}
+
 inline size_t exact_smem_bytes(int n, int f) {
   int L = f > 8 ? f - 8 : 0;
   return (size_t)(n * n + L * L) * sizeof(double);
