@@ -1,6 +1,6 @@
 // qb_batch.cuh -- many independent problems in one launch sequence.
 //
-// A batch of small problems (1 <= n <= 36) runs as six launches in total, whatever the
+// A batch of small problems (1 <= n <= 36) runs as five launches in total, whatever the
 // number of problems, with no host round trip in between:
 //   1. batch_gtab_kernel    G tables of every Gray-form problem (n >= 20)
 //   2. batch_gray_kernel    pass 1 of every Gray-form problem: one CTA per (problem, unit)
@@ -96,7 +96,7 @@ __global__ void batch_gtab_kernel(const BatchInst* __restrict__ insts, const Bat
   extern __shared__ double bgt_smem[];
   const BatchItem it = items[blockIdx.x];
   const BatchInst I = insts[it.inst];
-  gray_gtab_body(batch_problem(I, W), I.a, gtab + I.gtab_off, it.lo, it.hi, 0, blockDim.x >> 5, bgt_smem);
+  gray_gtab_body(batch_problem(I, W), I.a, gtab + I.gtab_off, it.lo, it.hi, bgt_smem);
 }
 
 // 2. pass 1: one CTA per item = (Gray problem, unit lo)

@@ -41,11 +41,14 @@ struct GrayParams {
 // per-state error bound of the fp32 path (see the header comment)
 inline double gray_error_bound(double abs_sum) { return 300.0 * abs_sum * 5.9604644775390625e-08; }
 
-// G(p)[c] for Gray steps i in [i_begin, i_end): one warp per step (warp w of the CTA takes
-// steps i_begin + first + w, + stride, ...), lane = c.  smem: gray_gtab_smem(n, a).
-__device__ __forceinline__ void gray_gtab_body(const ProblemDev& P, int a, float* __restrict__ gtab,
-                                               uint64_t i_begin, uint64_t i_end, uint64_t first, uint64_t stride,
-                                               double* gtab_smem) {
+// G(p)[c] for the Gray steps i in [lo, hi), lane = c.  The CTA's warps take contiguous
+// sub-ranges and walk them in Gray order: at the first step of a sub-range a warp computes
+// E_pre(p), the prefix fields h_l = sum_{m in p, m != l} W_lm (lane l < a) and
+// sum_{k in p} beta_k[c] from scratch in FP64, then each step flips one prefix variable k:
+//   E_pre += s (W_kk + h_k),  sum beta += s beta_k[c],  h_l += s W_lk (l != k)
+// (s = +1 when k turns on).  smem: gray_gtab_smem(n, a).
+__device__ __forceinline__ void gray_gtab_body(const ProblemDev& P, int a, float* __restrict__ gtab, uint64_t lo,
+                                               uint64_t hi, double* gtab_smem) {
   const int n = P.n;
   double* Ws = gtab_smem;      // n*n
   double* beta = Ws + n * n;   // a * 32
@@ -59,31 +62,42 @@ __device__ __forceinline__ void gray_gtab_body(const ProblemDev& P, int a, float
     beta[i] = s;
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  for (uint64_t i = i_begin + first + (threadIdx.x >> 5); i < i_end; i += stride) {
-    const uint64_t p = gray64(i);
-    // E_pre(p): lane handles prefix variables lane and lane + 32
-    double ep = 0.0;
-    for (int k = lane; k < a; k += 32) {
-      if (!((p >> (a - 1 - k)) & 1)) continue;
-      const double* row = Ws + k * n;
-      ep += row[k];
-      for (int m = 0; m < k; ++m)
-        if ((p >> (a - 1 - m)) & 1) ep += row[m];
-    }
-    for (int off = 16; off; off >>= 1) ep += __shfl_xor_sync(0xffffffffu, ep, off);
-    double g = ep;
-    for (int k = 0; k < a; ++k)
-      if ((p >> (a - 1 - k)) & 1) g += beta[k * 32 + lane];
-    gtab[i * 32 + lane] = (float)g;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint64_t len = (hi - lo + nw - 1) / nw;
+  const uint64_t w0 = lo + (uint64_t)warp * len;
+  const uint64_t w1 = min(hi, w0 + len);
+  if (w0 >= w1) return;  // uniform per warp
+  const uint64_t p0 = gray64(w0);
+  double h = 0.0, ep = 0.0, bs = 0.0;
+  if (lane < a) {
+    const double* row = Ws + lane * n;
+    for (int m = 0; m < a; ++m)
+      if (m != lane && ((p0 >> (a - 1 - m)) & 1)) h += row[m];
+    if ((p0 >> (a - 1 - lane)) & 1) ep = row[lane] + 0.5 * h;  // E_pre = sum_k in p (W_kk + h_k / 2)
+  }
+  for (int off = 16; off; off >>= 1) ep += __shfl_xor_sync(0xffffffffu, ep, off);
+  for (int k = 0; k < a; ++k)
+    if ((p0 >> (a - 1 - k)) & 1) bs += beta[k * 32 + lane];
+  gtab[w0 * 32 + lane] = (float)(ep + bs);
+  for (uint64_t i = w0 + 1; i < w1; ++i) {
+    const int kb = __ffsll((long long)i) - 1;
+    const int k = a - 1 - kb;
+    const double sg = ((gray64(i) >> kb) & 1) ? 1.0 : -1.0;
+    const double hk = __shfl_sync(0xffffffffu, h, k);
+    ep += sg * (Ws[k * n + k] + hk);
+    bs += sg * beta[k * 32 + lane];
+    if (lane < a && lane != k) h += sg * Ws[lane * n + k];
+    gtab[i * 32 + lane] = (float)(ep + bs);
   }
 }
 
 __global__ void gray_gtab_kernel(ProblemDev P, int a, int b, float* __restrict__ gtab) {
   extern __shared__ double gtab_smem[];
   (void)b;
-  gray_gtab_body(P, a, gtab, 0, 1ull << a, (uint64_t)blockIdx.x * (blockDim.x >> 5),
-                 (uint64_t)gridDim.x * (blockDim.x >> 5), gtab_smem);
+  const uint64_t steps = 1ull << a;
+  const uint64_t per = (steps + gridDim.x - 1) / gridDim.x;
+  const uint64_t lo = (uint64_t)blockIdx.x * per;
+  gray_gtab_body(P, a, gtab, min(lo, steps), min(lo + per, steps), gtab_smem);
 }
 
 inline size_t gray_gtab_smem(int n, int a) { return (size_t)(n * n + a * 32) * sizeof(double); }
