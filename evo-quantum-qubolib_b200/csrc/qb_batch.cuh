@@ -1,9 +1,11 @@
 // qb_batch.cuh -- many independent problems in one launch sequence.
 //
-// A batch of small problems (1 <= n <= 36) runs as five launches in total, whatever the
+// A batch of small problems (1 <= n <= 36) runs as six launches in total, whatever the
 // number of problems, with no host round trip in between:
-//   1. batch_gtab_kernel    G tables of every Gray-form problem (n >= 20)
+//   1. batch_gtab_kernel    G tables of every Gray-form problem (20 <= n < 24)
 //   2. batch_gray_kernel    pass 1 of every Gray-form problem: one CTA per (problem, unit)
+//   2'. tc_pass1_kernel     pass 1 of every tensor-core problem (n >= 24): each persistent
+//                           CTA runs a list of (problem, run of record blocks) items
 //   3. batch_select_kernel  per problem: smallest record, threshold, candidate records
 //   4. batch_exact_kernel   exact FP64 re-evaluation of every candidate record -- and, for
 //                           problems with n < 20, of all their records (the whole search)
@@ -18,12 +20,16 @@
 namespace qb {
 
 constexpr int kBatchGray = 1;   // Gray form + exact pass 2
+constexpr int kBatchTC = 2;     // tensor-core form + exact pass 2
 constexpr int kBatchExact = 3;  // exact enumeration of every record (small n)
 
 struct BatchInst {
   int n, kind;
   int a, b, cbbits, sbits, gubits;  // Gray plan
   int fbits;                        // exact plan: states per record = 2^fbits
+  int gl;                           // tensor-core plan: log2 tiles per record block
+  int exact_digits;                 // tensor-core plan: integer digits (exact)
+  double scale;                     // tensor-core plan: power of two applied to W
   int A, B;                         // QBF tie rule split (A inverse-Gray ranked prefix bits)
   int natural;                      // 1: natural order (smallest X) among ties
   int is_int;
@@ -76,7 +82,10 @@ __device__ __forceinline__ TieRule batch_rule(const BatchInst& I) {
 __device__ __forceinline__ RecGeom batch_geom(const BatchInst& I) {
   RecGeom g{};
   g.n = I.n;
-  if (I.kind == kBatchGray) {
+  if (I.kind == kBatchTC) {
+    g.kind = kGeomTC;
+    g.gl = I.gl;
+  } else if (I.kind == kBatchGray) {
     g.kind = kGeomGray;
     g.a = I.a;
     g.b = I.b;
@@ -119,7 +128,7 @@ batch_gray_kernel(const BatchInst* __restrict__ insts, const BatchItem* __restri
   gray_unit_body(g, it.lo, bgr_smem);
 }
 
-// 3. per Gray problem (one CTA each): pass-1 minimum, threshold, candidate records
+// 3. per Gray or tensor-core problem (one CTA each): pass-1 minimum, threshold, candidate records
 __global__ void batch_select_kernel(const BatchInst* __restrict__ insts, const uint32_t* __restrict__ gray_ids,
                                     const float* __restrict__ rec, BatchCand* __restrict__ cand,
                                     int* __restrict__ cand_count, int cap, float* __restrict__ pass1_min,

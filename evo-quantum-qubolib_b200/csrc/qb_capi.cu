@@ -98,7 +98,8 @@ struct qb_handle_s {
   cudaStream_t own = nullptr;
   cudaStream_t st = nullptr;
   DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
-  DevBuf bat[10];  // qb_solve_batch: W, insts, gtab items, unit items, gray ids, cands, out, G tables, records, minima
+  DevBuf bat[14];  // qb_solve_batch: W, insts, gtab items, unit items, selection ids, cands, out, G tables,
+                   // records, minima, scaled W, tensor-core items, item ranges, error word
   HostBuf hW, hmisc, hout;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // 4, 5: main kernel
   int64_t h2d = 0, d2h = 0;  // bytes copied by the current call
@@ -908,6 +909,7 @@ int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* 
 namespace {
 
 constexpr int kBatchMaxN = 36;            // larger problems are solved one by one
+constexpr int kBatchTcMinN = 24;          // from here on the tensor-core form (>= 512 tiles)
 constexpr uint64_t kBatchGtabChunk = 1024;  // G-table steps per CTA
 
 template <class T>
@@ -940,10 +942,15 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   std::vector<qb::BatchInst> insts(m);
   std::vector<double> Wall;
   std::vector<qb::BatchItem> gitems, uitems;
-  std::vector<uint32_t> gray_ids;
+  std::vector<uint32_t> gray_ids;  // problems with a selection step (Gray and tensor-core forms)
   std::vector<qb::BatchCand> pre;
+  std::vector<double> Wtc;                    // scaled W of the tensor-core problems
+  std::vector<std::pair<int, uint64_t>> tcs;  // (problem, offset in Wtc)
   uint64_t gtab_total = 0, rec_total = 0;
   size_t sm_gtab = 0, sm_gray = 0, sm_exact = 0;
+  int n_tc_max = 0;
+  bool any_gray = false;
+  const bool tc_allowed = o->form == QB_FORM_AUTO || o->form == QB_FORM_TC;
   for (int j = 0; j < m; ++j) {
     const qb_problem* p = &problems[ids[j]];
     std::vector<double> W;
@@ -964,7 +971,24 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     I.w_off = Wall.size();
     Wall.insert(Wall.end(), W.begin(), W.end());
     int free_bits;
-    if (n >= 20) {
+    if (n >= kBatchTcMinN && tc_allowed && qb::tc_supported(n)) {
+      qb::TcPlan tp;
+      qb::tc_plan(n, is_int, abs_sum, 0, 1, &tp);
+      I.kind = qb::kBatchTC;
+      I.gl = tp.gl;
+      I.exact_digits = tp.exact ? 1 : 0;
+      I.scale = tp.scale;
+      I.nrec = tp.rec_count;
+      I.eps = tp.eps;
+      I.rec_off = rec_total;
+      rec_total += I.nrec;
+      tcs.emplace_back(j, (uint64_t)Wtc.size());
+      for (double v : W) Wtc.push_back(v * tp.scale);
+      gray_ids.push_back((uint32_t)j);
+      n_tc_max = std::max(n_tc_max, n);
+      free_bits = I.gl + 12;
+    } else if (n >= 20) {
+      any_gray = true;
       I.kind = qb::kBatchGray;
       I.b = std::max(13, n - 16);
       I.a = n - I.b;
@@ -1028,7 +1052,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   qb::ExactOut* dO = static_cast<qb::ExactOut*>(B[6].p);
   QB_CUDA(cudaEventRecord(h->ev[0], h->st));
   QB_CUDA(cudaEventRecord(h->ev[4], h->st));
-  if (!gray_ids.empty()) {
+  if (any_gray) {
     QB_CUDA(cudaFuncSetAttribute(qb::batch_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gtab));
     qb::batch_gtab_kernel<<<(unsigned)gitems.size(), 256, sm_gtab, h->st>>>(
         dI, static_cast<const qb::BatchItem*>(B[2].p), dW, static_cast<float*>(B[7].p));
@@ -1037,6 +1061,65 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
         dI, static_cast<const qb::BatchItem*>(B[3].p), dW, static_cast<const float*>(B[7].p),
         static_cast<float*>(B[8].p));
     h->kernels += 2;
+  }
+  unsigned* tc_err = nullptr;
+  if (!tcs.empty()) {
+    // the tensor-core problems' record blocks, dealt out as contiguous runs to one persistent
+    // CTA per SM (a run may span problems: one item per problem piece)
+    uint64_t total = 0;
+    for (auto& t : tcs) total += 1ull << (insts[t.first].n - 15 - insts[t.first].gl);
+    const uint64_t ctas = std::min<uint64_t>((uint64_t)h->sm_count, total);
+    const uint64_t per = (total + ctas - 1) / ctas;
+    std::vector<qb::TcItem> items;
+    std::vector<std::pair<uint64_t, uint64_t>> offs;  // (scaled-W offset, record offset) per item
+    std::vector<uint32_t> first(1, 0);
+    uint64_t left = per;
+    for (auto& t : tcs) {
+      const qb::BatchInst& I = insts[t.first];
+      const uint64_t groups = 1ull << (I.n - 15 - I.gl);
+      uint64_t g = 0;
+      while (g < groups) {
+        const uint64_t take = std::min(left, groups - g);
+        qb::TcItem it{};
+        offs.emplace_back(t.second, I.rec_off + (g << 3));
+        it.i_begin = g << I.gl;
+        it.ntiles = take << I.gl;
+        it.n = I.n;
+        it.gl = I.gl;
+        it.exact = I.exact_digits;
+        it.inv_scale = (float)(1.0 / I.scale);
+        items.push_back(it);
+        g += take;
+        left -= take;
+        if (left == 0) {
+          first.push_back((uint32_t)items.size());
+          left = per;
+        }
+      }
+    }
+    if (first.back() != (uint32_t)items.size()) first.push_back((uint32_t)items.size());
+    // device addresses
+    QB_CUDA(B[10].ensure(std::max<size_t>(Wtc.size(), 1) * sizeof(double)));
+    for (size_t k = 0; k < items.size(); ++k) {
+      items[k].W = static_cast<const double*>(B[10].p) + offs[k].first;
+      items[k].rec = static_cast<float*>(B[8].p) + offs[k].second;
+    }
+    if ((rc = upload_vec(h, B[10], Wtc))) return rc;
+    if ((rc = upload_vec(h, B[11], items))) return rc;
+    if ((rc = upload_vec(h, B[12], first))) return rc;
+    QB_CUDA(B[13].ensure(16));
+    tc_err = static_cast<unsigned*>(B[13].p);
+    QB_CUDA(cudaMemsetAsync(tc_err, 0, 16, h->st));
+    qb::TcParams P{};
+    P.items = static_cast<const qb::TcItem*>(B[11].p);
+    P.item_first = static_cast<const uint32_t*>(B[12].p);
+    P.n_max = n_tc_max;
+    P.err = tc_err;
+    const qb::TcSmemLayout L = qb::tc_layout(n_tc_max);
+    const size_t smem = std::max<size_t>(L.total, 120 * 1024) + 1024;
+    QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, smem, h->st>>>(P);
+    ++h->kernels;
   }
   QB_CUDA(cudaEventRecord(h->ev[5], h->st));
   QB_CUDA(cudaEventRecord(h->ev[1], h->st));
@@ -1062,6 +1145,12 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   const uint64_t* hk = he + m;
   const float* hp = reinterpret_cast<const float*>(hk + m);
   const int got = *reinterpret_cast<const int*>(reinterpret_cast<const char*>(h->hout.p) + 2 * mb + (size_t)m * 4);
+  if (tc_err) {
+    unsigned e = 0;
+    QB_CUDA(cudaMemcpy(&e, tc_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    h->d2h += (int64_t)sizeof(unsigned);
+    if (e & qb::kErrTimeout) return QB_ETIMEOUT;
+  }
   if (got > cap) {
     *overflow = true;
     return QB_OK;
@@ -1084,10 +1173,10 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     R.best_e = qb::unord_f64(he[j]);
     R.best_e_int = I.is_int ? (int64_t)llround(R.best_e) : 0;
     R.order_key = key;
-    R.pass1_min = I.kind == qb::kBatchGray ? (double)hp[j] : R.best_e;
+    R.pass1_min = I.kind != qb::kBatchExact ? (double)hp[j] : R.best_e;
     R.err_bound = I.eps;
     R.states = (int64_t)1 << I.n;
-    R.form_used = I.kind == qb::kBatchGray ? QB_FORM_GRAY : QB_FORM_EXACT;
+    R.form_used = I.kind == qb::kBatchGray ? QB_FORM_GRAY : (I.kind == qb::kBatchTC ? QB_FORM_TC : QB_FORM_EXACT);
     R.is_integer = I.is_int;
     R.found = 1;
     R.status = QB_OK;

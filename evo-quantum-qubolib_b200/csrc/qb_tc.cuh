@@ -76,8 +76,18 @@ struct TcPlan {
   bool stall = false;      // test hook: the tile walk publishes nothing (waits expire)
 };
 
+// one CTA work item: a contiguous run of whole record blocks of one problem
+struct TcItem {
+  const double* W;     // scaled W of the problem, n*n
+  float* rec;          // record 0 of the item's first block
+  uint64_t i_begin;    // Gray index of the item's first tile (a multiple of 2^gl)
+  uint64_t ntiles;     // tiles in the item (a multiple of 2^gl, below 2^31)
+  int n, gl, exact;
+  float inv_scale;     // 1 / scale of W
+};
+
 struct TcParams {
-  int n, nt, gl;
+  int n, nt, gl;            // one problem (items == nullptr) ...
   int stall;
   int exact;
   float inv_scale;
@@ -86,6 +96,9 @@ struct TcParams {
   uint64_t groups;          // record blocks (2^gl tiles each) in this shard
   uint64_t groups_per_cta;  // contiguous blocks per CTA (last CTA may have fewer)
   float* rec;               // rec[0] = record (tile_begin >> gl) << 3
+  const TcItem* items;      // ... or a list of work items: CTA b runs items
+  const uint32_t* item_first;  //     [item_first[b], item_first[b + 1])
+  int n_max;                // largest n among the items (shared-memory layout)
   unsigned* err;            // error word
 };
 
@@ -291,11 +304,13 @@ __host__ __device__ inline TcSmemLayout tc_layout(int n) {
   return L;
 }
 
+// kItems = false: one problem (one work item per CTA, compiled without the item loop's
+// bookkeeping); kItems = true: the CTA's list of work items.
+template <bool kItems>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  const int n = P.n, nt = P.nt;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const TcSmemLayout L = tc_layout(n);
+  const TcSmemLayout L = tc_layout(kItems ? P.n_max : P.n);  // only the W block grows with n
   unsigned char* Asm = tc_smem + L.a_off;
   unsigned char* Bsm = tc_smem + L.b_off;
   uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + L.bar_off);
@@ -314,20 +329,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
   double* Ws = reinterpret_cast<double*>(tc_smem + L.w_off);
 
-  // this CTA's blocks of 2^gl tiles (Gray indices)
-  const uint64_t g0 = (uint64_t)blockIdx.x * P.groups_per_cta;
-  if (g0 >= P.groups) return;  // uniform per CTA
-  const uint64_t g1 = min(P.groups, g0 + P.groups_per_cta);
-  const uint64_t i_begin = P.tile_begin + (g0 << P.gl);
-  const uint64_t ntiles = (g1 - g0) << P.gl;  // a multiple of 32
-  const uint64_t t0 = gray64(i_begin);
-  const float s1 = P.exact ? 2048.0f : 1.0f;
-  // variables: t bit k <-> n-16-k, y bit i <-> n-9-i, u bit j <-> n-1-j
+  // this CTA's work: one run of record blocks of one problem, or a list of items
+  uint32_t it_lo = 0, it_hi = 1;
+  TcItem one{};
+  if (kItems) {
+    it_lo = P.item_first[blockIdx.x];
+    it_hi = P.item_first[blockIdx.x + 1];
+    if (it_lo >= it_hi) return;  // uniform per CTA
+  } else {
+    const uint64_t g0 = (uint64_t)blockIdx.x * P.groups_per_cta;
+    if (g0 >= P.groups) return;  // uniform per CTA
+    const uint64_t g1 = min(P.groups, g0 + P.groups_per_cta);
+    one = TcItem{P.W, P.rec + (g0 << 3), P.tile_begin + (g0 << P.gl), (g1 - g0) << P.gl, P.n, P.gl, P.exact,
+                 P.inv_scale};
+  }
 
-  // ---------------------------------------------------------------- set-up
-  for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
-  // this CTA's records start at +inf (the epilogue folds into them with atomic minima)
-  for (uint64_t r = (g0 << 3) + (uint64_t)tid; r < (g1 << 3); r += kTcThreads) P.rec[r] = __int_as_float(0x7f800000);
+  // ---------------------------------------------------------------- one-time set-up
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
       mbar_init(&p_full[s], 1);
@@ -348,295 +365,328 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  __syncthreads();
-  // A operand (constant)
-  for (int e = tid; e < 128 * 16; e += kTcThreads) {
-    int y = e >> 4, k = e & 15;
-    float v;
-    if (k < 14)
-      v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
-    else
-      v = (k & 1) ? s1 : 1.0f;
-    *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
-  }
-  // B operand, coupling columns (same in every stage)
-  for (int e = tid; e < kTcN * 7; e += kTcThreads) {
-    int u = e / 7, i = e % 7;
-    const double* row = Ws + (n - 9 - i) * n;
-    double v = 0.0;
-    for (int j = 0; j < 8; ++j)
-      if ((u >> j) & 1) v += row[n - 1 - j];
-    __half2 dg = digits((float)v, P.exact);
-    for (int s = 0; s < kTcBStages; ++s)
-      *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
-  }
-  // E_U(u)
-  for (int u = tid; u < kTcN; u += kTcThreads) {
-    double e = 0.0;
-    for (int j = 0; j < 8; ++j) {
-      if (!((u >> j) & 1)) continue;
-      const double* row = Ws + (n - 1 - j) * n;
-      e += row[n - 1 - j];
-      for (int j2 = 0; j2 < j; ++j2)
-        if ((u >> j2) & 1) e += row[n - 1 - j2];
-    }
-    EU[u] = (float)e;
-  }
-  // E_Y(y)
-  for (int y = tid; y < 128; y += kTcThreads) {
-    double e = 0.0;
-    for (int i = 0; i < 7; ++i) {
-      if (!((y >> i) & 1)) continue;
-      const double* row = Ws + (n - 9 - i) * n;
-      e += row[n - 9 - i];
-      for (int i2 = 0; i2 < i; ++i2)
-        if ((y >> i2) & 1) e += row[n - 9 - i2];
-    }
-    EY[y] = (float)e;
-  }
-  // t_lo tables: LO[p*16 + j] = (p^T W_TlU)_j (j < 8), LO[p*16 + 8 + i] = (p^T W_TlY)_i
-  // (i < 7), LO[p*16 + 15] = energy of the t_lo bits p
-  for (int e = tid; e < 32 * 16; e += kTcThreads) {
-    const int p = e >> 4, c = e & 15;
-    double v = 0.0;
-    if (c == 15) {
-      for (int k = 0; k < 5; ++k) {
-        if (!((p >> k) & 1)) continue;
-        const double* row = Ws + (n - 16 - k) * n;
-        v += row[n - 16 - k];
-        for (int k2 = 0; k2 < k; ++k2)
-          if ((p >> k2) & 1) v += row[n - 16 - k2];
-      }
-    } else {
-      const int col = c < 8 ? n - 1 - c : n - 9 - (c - 8);
-      for (int k = 0; k < 5; ++k)
-        if ((p >> k) & 1) v += Ws[(n - 16 - k) * n + col];
-    }
-    LO[e] = v;
-  }
-  fence_proxy_async();  // A / B stores (generic proxy) -> visible to tcgen05.mma
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  // Every role walks the CTA's tiles in the same order; barrier slots, stages and phases
+  // follow the CTA-wide tile counter jbase + local index across items.  Between items all
+  // roles meet at a CTA barrier with the pipelines empty (the MMA thread waits for its last
+  // MMA), so the per-item tables and B operand columns can be rewritten.
+  uint32_t jbase = 0;
+  for (uint32_t it = it_lo; it < (kItems ? it_hi : 1u); ++it) {
+    const TcItem I = kItems ? P.items[it] : one;
+    const int n = I.n, nt = n - 15, gl = I.gl, exact = I.exact;
+    const float inv_scale = I.inv_scale;
+    const uint64_t i_begin = I.i_begin, ntiles = I.ntiles;
+    float* rec = I.rec;
+    const uint64_t t0 = gray64(i_begin);
+    const float s1 = exact ? 2048.0f : 1.0f;
+    // variables: t bit k <-> n-16-k, y bit i <-> n-9-i, u bit j <-> n-1-j
 
-  bool ok = true;
-  if (warp == 0 && P.stall) {
-    // test hook (QB_FLAG_TEST_STALL): no tile parameters are published, so every other
-    // role's bounded wait runs out; the CTA drains and the host reports QB_ETIMEOUT
-  } else if (warp == 0) {
-    // ---------------------------------------------------------- tile walk
-    // Every lane keeps the t_hi state (fp64, lane-redundant): fh = t_hi^T W_ThU, gh =
-    // t_hi^T W_ThY, eh = E(t_hi), c_k = coupling of t_lo bit k with t_hi; lane l also
-    // keeps the fields of t_hi bits l and l + 32 from the other t_hi bits.
-    const int nh = nt - 5;  // t_hi bits: t bit 5 + m <-> variable n-21-m
-    double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) fh[k] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) gh[k] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) c[k] = 0.0;
-    const uint64_t th0 = t0 >> 5;
-    for (int m = 0; m < nh; ++m) {
-      if (!((th0 >> m) & 1)) continue;
-      const double* row = Ws + (n - 21 - m) * n;
-      eh += row[n - 21 - m];
-      for (int m2 = 0; m2 < m; ++m2)
-        if ((th0 >> m2) & 1) eh += row[n - 21 - m2];
-      if (lane < nh && lane != m) h0 += row[n - 21 - lane];
-      if (lane + 32 < nh && lane + 32 != m) h1 += row[n - 21 - lane - 32];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) fh[k] += row[n - 1 - k];
-#pragma unroll
-      for (int k = 0; k < 7; ++k) gh[k] += row[n - 9 - k];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) c[k] += row[n - 16 - k];
+    // ------------------------------------------------------------ per-item set-up
+    for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = I.W[i];
+    // the item's records start at +inf (the epilogue folds into them with atomic minima)
+    for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
+    __syncthreads();
+    // A operand (constant)
+    for (int e = tid; e < 128 * 16; e += kTcThreads) {
+      int y = e >> 4, k = e & 15;
+      float v;
+      if (k < 14)
+        v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
+      else
+        v = (k & 1) ? s1 : 1.0f;
+      *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
     }
-    for (uint64_t j0 = 0; j0 < ntiles && ok; j0 += 32) {
-      const uint64_t i0 = i_begin + j0;
-      if (j0 > 0) {  // t_hi changes by one bit between aligned runs of 32 Gray tiles
-        const int kb = __ffsll((long long)i0) - 1;  // >= 5
-        const int m = kb - 5;
-        const double sg = ((gray64(i0) >> kb) & 1) ? 1.0 : -1.0;
-        const double hm = __shfl_sync(0xffffffffu, m < 32 ? h0 : h1, m & 31);
-        const double* row = Ws + (n - 21 - m) * n;
-        eh += sg * (row[n - 21 - m] + hm);
-        if (lane < nh && lane != m) h0 += sg * row[n - 21 - lane];
-        if (lane + 32 < nh && lane + 32 != m) h1 += sg * row[n - 21 - lane - 32];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) fh[k] += sg * row[n - 1 - k];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) gh[k] += sg * row[n - 9 - k];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) c[k] += sg * row[n - 16 - k];
+    // B operand, coupling columns (same in every stage)
+    for (int e = tid; e < kTcN * 7; e += kTcThreads) {
+      int u = e / 7, i = e % 7;
+      const double* row = Ws + (n - 9 - i) * n;
+      double v = 0.0;
+      for (int j = 0; j < 8; ++j)
+        if ((u >> j) & 1) v += row[n - 1 - j];
+      __half2 dg = digits((float)v, exact);
+      for (int s = 0; s < kTcBStages; ++s)
+        *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+    }
+    // E_U(u)
+    for (int u = tid; u < kTcN; u += kTcThreads) {
+      double e = 0.0;
+      for (int j = 0; j < 8; ++j) {
+        if (!((u >> j) & 1)) continue;
+        const double* row = Ws + (n - 1 - j) * n;
+        e += row[n - 1 - j];
+        for (int j2 = 0; j2 < j; ++j2)
+          if ((u >> j2) & 1) e += row[n - 1 - j2];
       }
-      // this lane's tile
-      const uint64_t j = j0 + (uint64_t)lane;
-      const int tl = (int)(gray64(i0 + (uint64_t)lane) & 31ull);
-      const double* lo = LO + tl * 16;
-      double et = eh + lo[15];
-#pragma unroll
-      for (int k = 0; k < 5; ++k)
-        if ((tl >> k) & 1) et += c[k];
-      const int s = (int)(j % kTcParamSlots);
-      ok = mbar_wait(&p_empty[s], (uint32_t)(((j / kTcParamSlots) & 1) ^ 1), abort_flag);
-      ok = __all_sync(0xffffffffu, ok);  // keep the warp converged for the next shuffle
-      if (!ok) break;
-      TcSlot& sl = slots[s];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) sl.f[k] = (float)(fh[k] + lo[k]);
-#pragma unroll
-      for (int k = 0; k < 7; ++k) sl.g[k] = (float)(gh[k] + lo[8 + k]);
-      sl.et = (float)et;
-      mbar_arrive(&p_full[s]);
+      EU[u] = (float)e;
     }
-  } else if (warp == 1) {
-    // ---------------------------------------------------------- MMA issue
-    if (lane == 0) {
-      const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
+    // E_Y(y)
+    for (int y = tid; y < 128; y += kTcThreads) {
+      double e = 0.0;
+      for (int i = 0; i < 7; ++i) {
+        if (!((y >> i) & 1)) continue;
+        const double* row = Ws + (n - 9 - i) * n;
+        e += row[n - 9 - i];
+        for (int i2 = 0; i2 < i; ++i2)
+          if ((y >> i2) & 1) e += row[n - 9 - i2];
+      }
+      EY[y] = (float)e;
+    }
+    // t_lo tables: LO[p*16 + j] = (p^T W_TlU)_j (j < 8), LO[p*16 + 8 + i] = (p^T W_TlY)_i
+    // (i < 7), LO[p*16 + 15] = energy of the t_lo bits p
+    for (int e = tid; e < 32 * 16; e += kTcThreads) {
+      const int p = e >> 4, c = e & 15;
+      double v = 0.0;
+      if (c == 15) {
+        for (int k = 0; k < 5; ++k) {
+          if (!((p >> k) & 1)) continue;
+          const double* row = Ws + (n - 16 - k) * n;
+          v += row[n - 16 - k];
+          for (int k2 = 0; k2 < k; ++k2)
+            if ((p >> k2) & 1) v += row[n - 16 - k2];
+        }
+      } else {
+        const int col = c < 8 ? n - 1 - c : n - 9 - (c - 8);
+        for (int k = 0; k < 5; ++k)
+          if ((p >> k) & 1) v += Ws[(n - 16 - k) * n + col];
+      }
+      LO[e] = v;
+    }
+    fence_proxy_async();  // A / B stores (generic proxy) -> visible to tcgen05.mma
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+
+    bool ok = true;
+    if (warp == 0 && P.stall) {
+      // test hook (QB_FLAG_TEST_STALL): no tile parameters are published, so every other
+      // role's bounded wait runs out; the CTA drains and the host reports QB_ETIMEOUT
+    } else if (warp == 0) {
+      // ---------------------------------------------------------- tile walk
+      // Every lane keeps the t_hi state (fp64, lane-redundant): fh = t_hi^T W_ThU, gh =
+      // t_hi^T W_ThY, eh = E(t_hi), c_k = coupling of t_lo bit k with t_hi; lane l also
+      // keeps the fields of t_hi bits l and l + 32 from the other t_hi bits.
+      const int nh = nt - 5;  // t_hi bits: t bit 5 + m <-> variable n-21-m
+      double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fh[k] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) gh[k] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) c[k] = 0.0;
+      const uint64_t th0 = t0 >> 5;
+      for (int m = 0; m < nh; ++m) {
+        if (!((th0 >> m) & 1)) continue;
+        const double* row = Ws + (n - 21 - m) * n;
+        eh += row[n - 21 - m];
+        for (int m2 = 0; m2 < m; ++m2)
+          if ((th0 >> m2) & 1) eh += row[n - 21 - m2];
+        if (lane < nh && lane != m) h0 += row[n - 21 - lane];
+        if (lane + 32 < nh && lane + 32 != m) h1 += row[n - 21 - lane - 32];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) fh[k] += row[n - 1 - k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gh[k] += row[n - 9 - k];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) c[k] += row[n - 16 - k];
+      }
+      for (uint64_t j0 = 0; j0 < ntiles && ok; j0 += 32) {
+        const uint64_t i0 = i_begin + j0;
+        if (j0 > 0) {  // t_hi changes by one bit between aligned runs of 32 Gray tiles
+          const int kb = __ffsll((long long)i0) - 1;  // >= 5
+          const int m = kb - 5;
+          const double sg = ((gray64(i0) >> kb) & 1) ? 1.0 : -1.0;
+          const double hm = __shfl_sync(0xffffffffu, m < 32 ? h0 : h1, m & 31);
+          const double* row = Ws + (n - 21 - m) * n;
+          eh += sg * (row[n - 21 - m] + hm);
+          if (lane < nh && lane != m) h0 += sg * row[n - 21 - lane];
+          if (lane + 32 < nh && lane + 32 != m) h1 += sg * row[n - 21 - lane - 32];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) fh[k] += sg * row[n - 1 - k];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) gh[k] += sg * row[n - 9 - k];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) c[k] += sg * row[n - 16 - k];
+        }
+        // this lane's tile
+        const uint64_t j = j0 + (uint64_t)lane;
+        const int tl = (int)(gray64(i0 + (uint64_t)lane) & 31ull);
+        const double* lo = LO + tl * 16;
+        double et = eh + lo[15];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if ((tl >> k) & 1) et += c[k];
+        const uint64_t jg = jbase + j;
+        const int s = (int)(jg % kTcParamSlots);
+        ok = mbar_wait(&p_empty[s], (uint32_t)(((jg / kTcParamSlots) & 1) ^ 1), abort_flag);
+        ok = __all_sync(0xffffffffu, ok);  // keep the warp converged for the next shuffle
+        if (!ok) break;
+        TcSlot& sl = slots[s];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sl.f[k] = (float)(fh[k] + lo[k]);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) sl.g[k] = (float)(gh[k] + lo[8 + k]);
+        sl.et = (float)et;
+        mbar_arrive(&p_full[s]);
+      }
+    } else if (warp == 1) {
+      // ---------------------------------------------------------- MMA issue
+      if (lane == 0) {
+        const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
+        const uint32_t nt32 = (uint32_t)ntiles;
+        uint32_t issued = 0;
+        for (uint32_t jl = 0; jl < nt32 && ok; ++jl) {
+          const uint32_t j = jbase + jl;
+          const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
+          const uint32_t as = j & 1u;
+          ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag) &&
+               mbar_wait(&acc_empty[as], ((j >> 1) & 1u) ^ 1u, abort_flag);
+          if (!ok) break;
+          tc_fence_after();
+          // every epilogue warp has released tile j-2 (it read that tile's row terms before its
+          // release, and MMA j-2 completed before the tile could be read): its B stage is free
+          if (j >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(j - kTcStages) & (uint32_t)(kTcBStages - 1)]);
+          const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
+          tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc);
+          tc_commit(&acc_full[as]);  // one commit per MMA
+          issued = jl + 1;
+        }
+        if (issued) {  // the last MMA completes before the item's operands can change
+          const uint32_t j = jbase + issued - 1;
+          mbar_wait(&acc_full[j & 1u], (j >> 1) & 1u, abort_flag);
+        }
+      }
+      __syncwarp();
+    } else if (warp < 4) {
+      // ---------------------------------------------------------- B producers (C_t columns)
+      // warp 2 + (j & 1) fills tile j: rows u = lane + 32 r, r < 8 (u bits 5..7 = r)
+      // and the row terms R_t(y) = E_T(t) + E_Y(y) + (t^T W_TY) y of rows y = lane + 32 r, r < 4
       const uint32_t nt32 = (uint32_t)ntiles;
-      uint32_t issued = 0;
-      for (uint32_t j = 0; j < nt32 && ok; ++j) {
+      for (uint32_t jl = (uint32_t)(warp - 2); jl < nt32 && ok; jl += 2) {
+        const uint32_t j = jbase + jl;  // CTA-wide tile counter: slots, stages and phases
+        const uint32_t s = j & (uint32_t)(kTcParamSlots - 1);
         const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-        const uint32_t as = j & 1u;
-        ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag) &&
-             mbar_wait(&acc_empty[as], ((j >> 1) & 1u) ^ 1u, abort_flag);
+        ok = mbar_wait(&p_full[s], (j >> 6) & 1u, abort_flag);
+        if (!ok) break;
+        __half2 dg[8];
+        float rr[4];
+        {
+          const TcSlot& sl = slots[s];
+          float s5 = 0.f;
+#pragma unroll
+          for (int jb = 0; jb < 5; ++jb)
+            if ((lane >> jb) & 1) s5 += sl.f[jb];
+          const float f5 = sl.f[5], f6 = sl.f[6], f7 = sl.f[7];
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            float cr = s5;
+            if (r & 1) cr += f5;
+            if (r & 2) cr += f6;
+            if (r & 4) cr += f7;
+            dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+          }
+          float g5 = sl.et;
+#pragma unroll
+          for (int i = 0; i < 5; ++i)
+            if ((lane >> i) & 1) g5 += sl.g[i];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            float v = g5;
+            if (r & 1) v += sl.g[5];
+            if (r & 2) v += sl.g[6];
+            rr[r] = v + EY[lane + 32 * r];
+          }
+        }
+        ok = mbar_wait(&b_empty[bs], ((j >> 3) & 1u) ^ 1u, abort_flag);
+        if (!ok) break;
+        unsigned char* Bst = Bsm + bs * kTcN * 32;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) Rs[bs * 128 + lane + 32 * r] = rr[r];
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&b_full[bs]);
+          mbar_arrive(&p_empty[s]);
+        }
+      }
+    } else {
+      // ---------------------------------------------------------- epilogue
+      const int q = warp & 3;           // TMEM lane quarter (warp id % 4)
+      const int cq = (warp - 4) >> 2;   // 0..3: (tile parity, column half) below
+      const int y = q * 32 + lane;
+      const float inv = inv_scale;
+      const float inf = __int_as_float(0x7f800000);
+      float rmin = inf;
+      // warps 4-11 take the even tiles (accumulator stage 0), warps 12-19 the odd ones (stage 1),
+      // so the four warps sharing a scheduler work on different tiles and one stage's waits
+      // overlap the other stage's minima; each reads 128 columns (column half hh) in two
+      // 64-column rounds and releases the stage once the second round has landed
+      const uint32_t sp = (uint32_t)cq >> 1;   // tile parity = accumulator stage
+      const uint32_t hh = (uint32_t)cq & 1u;   // column half
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+      // 32-bit loop state (a CTA walks fewer than 2^32 tiles); records every 2^gl tiles (2^(gl-1)
+      // of this warp's parity), counted down from the CTA's first block (aligned to 2^gl)
+      const uint32_t nt32 = (uint32_t)ntiles;
+      uint32_t rec_left = 1u << (gl - 1);
+      uint64_t Jrec = 0;
+      for (uint32_t jl = sp; jl < nt32 && ok; jl += 2) {
+        const uint32_t j = jbase + jl;  // CTA-wide tile counter (jbase is even)
+        const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
+        // the B stage of tile j is full: its row terms are written (b_full cannot move on to
+        // tile j + 8 before this warp has released tile j)
+        ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag);
+        if (!ok) break;
+        const float R = Rs[bs * 128 + y];
+        ok = mbar_wait(&acc_full[sp], (j >> 1) & 1u, abort_flag);
         if (!ok) break;
         tc_fence_after();
-        // every epilogue warp has released tile j-2 (it read that tile's row terms before its
-        // release, and MMA j-2 completed before the tile could be read): its B stage is free
-        if (j >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(j - kTcStages) & (uint32_t)(kTcBStages - 1)]);
-        const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
-        tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc);
-        tc_commit(&acc_full[as]);  // one commit per MMA
-        issued = j + 1;
-      }
-      if (issued) {  // let the last MMA finish before the CTA can release TMEM
-        const uint32_t j = issued - 1;
-        mbar_wait(&acc_full[j & 1u], (j >> 1) & 1u, abort_flag);
-      }
-    }
-    __syncwarp();
-  } else if (warp < 4) {
-    // ---------------------------------------------------------- B producers (C_t columns)
-    // warp 2 + (j & 1) fills tile j: rows u = lane + 32 r, r < 8 (u bits 5..7 = r)
-    // and the row terms R_t(y) = E_T(t) + E_Y(y) + (t^T W_TY) y of rows y = lane + 32 r, r < 4
-    const uint32_t nt32 = (uint32_t)ntiles;
-    for (uint32_t j = (uint32_t)(warp - 2); j < nt32 && ok; j += 2) {
-      const uint32_t s = j & (uint32_t)(kTcParamSlots - 1);
-      const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-      ok = mbar_wait(&p_full[s], (j >> 6) & 1u, abort_flag);
-      if (!ok) break;
-      __half2 dg[8];
-      float rr[4];
-      {
-        const TcSlot& sl = slots[s];
-        float s5 = 0.f;
-#pragma unroll
-        for (int jb = 0; jb < 5; ++jb)
-          if ((lane >> jb) & 1) s5 += sl.f[jb];
-        const float f5 = sl.f[5], f6 = sl.f[6], f7 = sl.f[7];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          float cr = s5;
-          if (r & 1) cr += f5;
-          if (r & 2) cr += f6;
-          if (r & 4) cr += f7;
-          dg[r] = digits(EU[lane + 32 * r] + cr, P.exact);
-        }
-        float g5 = sl.et;
-#pragma unroll
-        for (int i = 0; i < 5; ++i)
-          if ((lane >> i) & 1) g5 += sl.g[i];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          float v = g5;
-          if (r & 1) v += sl.g[5];
-          if (r & 2) v += sl.g[6];
-          rr[r] = v + EY[lane + 32 * r];
+        uint32_t ra[32], rb[32];
+        QB_TC_LD32(tbase, ra);
+        QB_TC_LD32(tbase + 32, rb);
+        tc_wait_ld();
+        reg_fence32(ra);
+        reg_fence32(rb);
+        const float m1 = fminf(min32(ra), min32(rb));
+        QB_TC_LD32(tbase + 64, ra);
+        QB_TC_LD32(tbase + 96, rb);
+        tc_wait_ld();
+        reg_fence32(ra);
+        reg_fence32(rb);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[sp]);  // the stage is free once the data is in registers
+        const float m = fminf(m1, fminf(min32(ra), min32(rb)));
+        rmin = fminf(rmin, m + R);
+        if (--rec_left == 0) {
+          // both parities' warps of (column half, lane quarter) fold into one record
+          const float wm = warp_min_f(rmin) * inv;
+          if (lane == 0) {
+            float* dst = rec + ((Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+            if (wm >= 0.f)
+              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+            else
+              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+          }
+          ++Jrec;
+          rec_left = 1u << (gl - 1);
+          rmin = inf;
         }
       }
-      ok = mbar_wait(&b_empty[bs], ((j >> 3) & 1u) ^ 1u, abort_flag);
-      if (!ok) break;
-      unsigned char* Bst = Bsm + bs * kTcN * 32;
-#pragma unroll
-      for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) Rs[bs * 128 + lane + 32 * r] = rr[r];
-      fence_proxy_async();
-      __syncwarp();
-      if (lane == 0) {
-        mbar_arrive(&b_full[bs]);
-        mbar_arrive(&p_empty[s]);
-      }
     }
-  } else {
-    // ---------------------------------------------------------- epilogue
-    const int q = warp & 3;           // TMEM lane quarter (warp id % 4)
-    const int cq = (warp - 4) >> 2;   // 0..3: (tile parity, column half) below
-    const int y = q * 32 + lane;
-    const float inv = P.inv_scale;
-    const float inf = __int_as_float(0x7f800000);
-    float rmin = inf;
-    // warps 4-11 take the even tiles (accumulator stage 0), warps 12-19 the odd ones (stage 1),
-    // so the four warps sharing a scheduler work on different tiles and one stage's waits
-    // overlap the other stage's minima; each reads 128 columns (column half hh) in two
-    // 64-column rounds and releases the stage once the second round has landed
-    const uint32_t sp = (uint32_t)cq >> 1;   // tile parity = accumulator stage
-    const uint32_t hh = (uint32_t)cq & 1u;   // column half
-    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
-    // 32-bit loop state (a CTA walks fewer than 2^32 tiles); records every 2^gl tiles (2^(gl-1)
-    // of this warp's parity), counted down from the CTA's first block (aligned to 2^gl)
-    const uint32_t nt32 = (uint32_t)ntiles;
-    uint32_t rec_left = 1u << (P.gl - 1);
-    uint64_t Jrec = (i_begin - P.tile_begin) >> P.gl;
-    for (uint32_t j = sp; j < nt32 && ok; j += 2) {
-      const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-      // the B stage of tile j is full: its row terms are written (b_full cannot move on to
-      // tile j + 8 before this warp has released tile j)
-      ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag);
-      if (!ok) break;
-      const float R = Rs[bs * 128 + y];
-      ok = mbar_wait(&acc_full[sp], (j >> 1) & 1u, abort_flag);
-      if (!ok) break;
-      tc_fence_after();
-      uint32_t ra[32], rb[32];
-      QB_TC_LD32(tbase, ra);
-      QB_TC_LD32(tbase + 32, rb);
-      tc_wait_ld();
-      reg_fence32(ra);
-      reg_fence32(rb);
-      const float m1 = fminf(min32(ra), min32(rb));
-      QB_TC_LD32(tbase + 64, ra);
-      QB_TC_LD32(tbase + 96, rb);
-      tc_wait_ld();
-      reg_fence32(ra);
-      reg_fence32(rb);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[sp]);  // the stage is free once the data is in registers
-      const float m = fminf(m1, fminf(min32(ra), min32(rb)));
-      rmin = fminf(rmin, m + R);
-      if (--rec_left == 0) {
-        // both parities' warps of (column half, lane quarter) fold into one record
-        const float wm = warp_min_f(rmin) * inv;
-        if (lane == 0) {
-          float* dst = P.rec + ((Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
-          if (wm >= 0.f)
-            atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
-          else
-            atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
-        }
-        ++Jrec;
-        rec_left = 1u << (P.gl - 1);
-        rmin = inf;
-      }
+    if (!ok) {
+      *abort_flag = 1;
+      atomicOr(P.err, kErrTimeout);
     }
-  }
-  if (!ok) {
-    *abort_flag = 1;
-    atomicOr(P.err, kErrTimeout);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (!kItems) break;
+    jbase += (uint32_t)ntiles;
+    if (*abort_flag) break;  // uniform: read after the barrier
   }
   tc_fence_before();
   __syncthreads();
@@ -687,9 +737,10 @@ inline int tc_launch(const TcPlan& p, float* rec, void* scratch, cudaStream_t st
   const TcSmemLayout L = tc_layout(p.n);
   // at least 120 KB so that one CTA (and one 512-column TMEM allocation) runs per SM
   const size_t smem = std::max<size_t>(L.total, 120 * 1024) + 1024;
-  if (cudaFuncSetAttribute(tc_pass1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+  if (cudaFuncSetAttribute(tc_pass1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
     return 4;
-  tc_pass1_kernel<<<(unsigned)ctas, kTcThreads, smem, st>>>(P);
+  tc_pass1_kernel<false><<<(unsigned)ctas, kTcThreads, smem, st>>>(P);
   ++*kernels;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }
