@@ -21,6 +21,7 @@ struct ExactOut {
 
 constexpr int kExactThreads = 256;
 constexpr int kExactMaxFree = 40;
+constexpr int kExactTableMaxL = 12;  // walks of up to 12 bits use the table form below
 
 __device__ __forceinline__ double energy_from_scratch(const double* __restrict__ Ws, int n, uint64_t X) {
   double e = 0.0;
@@ -85,11 +86,72 @@ __device__ __forceinline__ void exact_record_body(const ProblemDev& P, const Tie
     Wl[i] = Ws[(n - 1 - pos[a]) * n + (n - 1 - pos[c])];
   }
   __syncthreads();
+  // Table form (walks of at most kExactTableMaxL bits, when the record's smem holds the
+  // tables): with the thread's other bits fixed in X0, the energy of X0 with the walked
+  // pattern g is E(X0) + a . g + q(g), where a_u is the field of walked variable u from X0
+  // (per thread, in smem) and q(g) the energy of the pattern alone (shared by all threads).
+  // A Gray walk then costs one field add, one table read and one add per state.
+  const bool table = L <= kExactTableMaxL && nfree - 8 <= kExactTableMaxL;
+  double* qt = Wl + L * L;                    // q(g), 2^L entries
+  double* at = qt + (table ? (1 << L) : 0);   // a_u of thread t at [u * blockDim.x + t]
+  if (table) {
+    for (int g = threadIdx.x; g < (1 << L); g += blockDim.x) {
+      double q = 0.0;
+      for (int u = 0; u < L; ++u) {
+        if (!((g >> u) & 1)) continue;
+        q += Wl[u * L + u];
+        for (int w = 0; w < u; ++w)
+          if ((g >> w) & 1) q += Wl[u * L + w];
+      }
+      qt[g] = q;
+    }
+    __syncthreads();
+  }
 
   double best_e = __longlong_as_double(0x7ff0000000000000ll);  // +inf
   uint64_t best_k = ~0ull, best_x = 0;
   const int t = threadIdx.x;
-  if (t < (1 << tb)) {
+  if (table && t < (1 << tb)) {
+    uint64_t X0 = base;
+    for (int j = 0; j < tb; ++j)
+      if ((t >> j) & 1) X0 |= 1ull << pos[L + j];
+    const double c0 = energy_from_scratch(Ws, n, X0);
+    for (int j = 0; j < L; ++j) {
+      const int v = n - 1 - pos[j];
+      double s = 0.0;
+      uint64_t rem = X0 & mask64(n);
+      while (rem) {
+        const int q = __ffsll((long long)rem) - 1;
+        rem &= rem - 1;
+        s += Ws[v * n + (n - 1 - q)];  // the walked bits are 0 in X0: no self term
+      }
+      at[j * blockDim.x + t] = s;
+    }
+    best_e = c0;
+    best_k = tie_key(R, X0);
+    best_x = X0;
+    double A = 0.0;
+    const uint32_t steps = 1u << L;
+    for (uint32_t st = 1; st < steps; ++st) {
+      const int j = __ffs(st) - 1;
+      const uint32_t g = st ^ (st >> 1);
+      const double aj = at[j * blockDim.x + t];
+      A = ((g >> j) & 1) ? A + aj : A - aj;
+      const double e = c0 + A + qt[g];
+      if (e <= best_e) {
+        uint64_t X = X0;
+        for (int u = 0; u < L; ++u)
+          if ((g >> u) & 1) X |= 1ull << pos[u];
+        const uint64_t k = tie_key(R, X);
+        if (lex_less(e, k, best_e, best_k)) {
+          best_e = e;
+          best_k = k;
+          best_x = X;
+        }
+      }
+    }
+    best_e = energy_from_scratch(Ws, n, best_x);
+  } else if (t < (1 << tb)) {
     uint64_t X = base;
     for (int j = 0; j < tb; ++j)
       if ((t >> j) & 1) X |= 1ull << pos[L + j];
@@ -242,7 +304,9 @@ __global__ void exact_final_kernel(const ExactOut* __restrict__ out, const int* 
 
 inline size_t exact_smem_bytes(int n, int f) {
   int L = f > 8 ? f - 8 : 0;
-  return (size_t)(n * n + L * L) * sizeof(double);
+  size_t d = (size_t)(n * n + L * L);
+  if (L <= kExactTableMaxL) d += ((size_t)1 << L) + (size_t)kExactThreads * L;  // q table, per-thread fields
+  return d * sizeof(double);
 }
 
 }  // namespace qb
