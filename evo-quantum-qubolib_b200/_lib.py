@@ -139,9 +139,11 @@ class Handle:
         Q = np.ascontiguousarray(Q)
         if Q.ndim != 2 or Q.shape[0] != Q.shape[1]:
             raise ValueError(f"Q must be square, got shape {Q.shape}")
-        if Q.dtype not in _DTYPES:
+        code = _DTYPES.get(Q.dtype)
+        if code is None:
             raise TypeError(f"unsupported Q dtype {Q.dtype}")
-        p = QbProblem(n=Q.shape[0], dtype=_DTYPES[Q.dtype], q=Q.ctypes.data, ldq=Q.shape[0], q_on_device=0)
+        n = Q.shape[0]
+        p = QbProblem(n, code, Q.__array_interface__["data"][0], n, 0, 0)
         return p, Q
 
     @staticmethod
@@ -211,7 +213,19 @@ class Handle:
         rc = load().qb_solve_batch(self._h, probs, len(Qs), ctypes.byref(o), res)
         if rc:
             _raise(rc, "qb_solve_batch")
-        return [result_dict(res[i], probs[i].n) for i in range(len(Qs))]
+        # decoded together: the results as one structured array, the state bits grouped by size
+        ns = np.array([q.shape[0] for q in keep], dtype=np.int64)
+        arr = np.frombuffer(res, dtype=np.dtype(QbResult))
+        xs = arr["best_x"].astype(np.uint64)
+        bits = [None] * len(Qs)
+        for n in np.unique(ns):
+            idx = np.flatnonzero(ns == n)
+            sh = np.arange(int(n) - 1, -1, -1, dtype=np.uint64)
+            mat = ((xs[idx][:, None] >> sh[None, :]) & np.uint64(1)).astype(np.int32)
+            for row, i in enumerate(idx):
+                bits[i] = mat[row]
+        names = [f[0] for f in QbResult._fields_]
+        return [_row_dict(dict(zip(names, row)), bits[i]) for i, row in enumerate(arr.tolist())]
 
     def prefix_minima(self, Q: np.ndarray, prefix_bits: int = -1) -> np.ndarray:
         """Per-prefix minimum energies in QBF's Gray visiting order (qb_prefix_minima)."""
@@ -256,6 +270,30 @@ def result_dict(r: QbResult, n: int) -> dict:
         "kernel_ms": float(r.kernel_ms),
         "h2d_bytes": int(r.h2d_bytes),
         "d2h_bytes": int(r.d2h_bytes),
+    }
+
+
+def _row_dict(f: dict, bits: np.ndarray) -> dict:
+    """result_dict of one row of a structured array of qb_result (field name -> value)."""
+    return {
+        "found": bool(f["found"]),
+        "best_X_int": int(f["best_x"]),
+        "best_X": bits,
+        "best_E": float(f["best_e"]),
+        "best_E_int": int(f["best_e_int"]),
+        "order_key": int(f["order_key"]),
+        "pass1_min": float(f["pass1_min"]),
+        "err_bound": float(f["err_bound"]),
+        "states": int(f["states"]),
+        "candidate_records": int(f["candidate_records"]),
+        "form": FORM_NAMES.get(int(f["form_used"]), str(f["form_used"])),
+        "is_integer": bool(f["is_integer"]),
+        "pass1_ms": float(f["pass1_ms"]),
+        "pass2_ms": float(f["pass2_ms"]),
+        "kernels": int(f["kernels"]),
+        "kernel_ms": float(f["kernel_ms"]),
+        "h2d_bytes": int(f["h2d_bytes"]),
+        "d2h_bytes": int(f["d2h_bytes"]),
     }
 
 
