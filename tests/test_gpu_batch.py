@@ -74,7 +74,7 @@ def test_batch_ties_follow_the_split(cuda_ok):
 
 def test_batch_natural_rule_and_large_member(cuda_ok):
     rng = np.random.default_rng(9)
-    Qs = [rng.integers(-3, 4, (n, n)).astype(np.int32) for n in (10, 21, 37)]
+    Qs = [rng.integers(-3, 4, (n, n)).astype(np.int32) for n in (10, 21, 25, 37)]
     res = _lib.handle(0).solve_batch(Qs, tie_rule="natural")
     for Q, r in zip(Qs, res):
         single = _lib.handle(0).solve(Q, tie_rule="natural")
@@ -109,4 +109,16 @@ def test_batch_cfg5_sample_of_4096(cuda_ok):
     Qs = [configs.batch_instance(i) for i in range(0, 4096, 128)]
     res = _lib.handle(0).solve_batch(Qs)
     for Q, r in zip(Qs, res):
+        _check(Q, r)
+
+
+def test_batch_tensor_core_members_beyond_exact_digits(cuda_ok):
+    """n >= 24 members take the tensor-core form; integers with sum |Q| > 2^22 use its
+    float digits and an error bound, the answers stay exact after re-evaluation."""
+    rng = np.random.default_rng(21)
+    Qs = [rng.integers(-100000, 100001, (n, n)).astype(np.int64) for n in (24, 25, 26)]
+    Qs += [rng.integers(-40, 41, (n, n)).astype(np.int16) for n in (24, 26)]
+    res = _lib.handle(0).solve_batch(Qs)
+    for Q, r in zip(Qs, res):
+        assert r["form"] == "tc"
         _check(Q, r)
