@@ -21,7 +21,7 @@
  *                                        prefixes, min over best_E + prefix_E
  *
  * Arithmetic: integer Q is accumulated exactly (int32 when sum|Q| < 2^31, else int64);
- * float Q in IEEE double (the FP64 semantics the GPU results are judged against).
+ * float Q in IEEE double (the FP64 semantics the GPU results are compared with).
  * The reference accumulates in Q's own dtype; where that dtype could wrap or round,
  * this port gives the exact / FP64 answer instead.
  *
