@@ -202,30 +202,49 @@ class Handle:
         return result_dict(r, n)
 
     def solve_batch(self, Qs: list, **opts) -> list[dict]:
-        probs = (QbProblem * len(Qs))()
-        keep = []
-        for i, Q in enumerate(Qs):
-            p, k = self._problem(Q)
-            probs[i] = p
-            keep.append(k)
+        count = len(Qs)
+        probs = (QbProblem * count)()
+        keep = [np.ascontiguousarray(Q) for Q in Qs]
+        for Q in keep:
+            if Q.ndim != 2 or Q.shape[0] != Q.shape[1]:
+                raise ValueError(f"Q must be square, got shape {Q.shape}")
+            if Q.dtype not in _DTYPES:
+                raise TypeError(f"unsupported Q dtype {Q.dtype}")
+        # the problem descriptors filled column by column through a structured view
+        ns = np.fromiter((q.shape[0] for q in keep), dtype=np.int64, count=count)
+        if count:
+            view = np.frombuffer(probs, dtype=np.dtype(QbProblem))
+            view["n"] = ns
+            view["ldq"] = ns
+            view["dtype"] = np.fromiter((_DTYPES[q.dtype] for q in keep), dtype=np.int32, count=count)
+            view["q"] = np.fromiter((q.__array_interface__["data"][0] for q in keep), dtype=np.uint64, count=count)
         o = self.options(**opts)
-        res = (QbResult * len(Qs))()
-        rc = load().qb_solve_batch(self._h, probs, len(Qs), ctypes.byref(o), res)
+        res = (QbResult * count)()
+        rc = load().qb_solve_batch(self._h, probs, count, ctypes.byref(o), res)
         if rc:
             _raise(rc, "qb_solve_batch")
-        # decoded together: the results as one structured array, the state bits grouped by size
-        ns = np.array([q.shape[0] for q in keep], dtype=np.int64)
+        if not count:
+            return []
+        # decoded together: one structured array, the state bits grouped by size
         arr = np.frombuffer(res, dtype=np.dtype(QbResult))
         xs = arr["best_x"].astype(np.uint64)
-        bits = [None] * len(Qs)
+        bits = [None] * count
         for n in np.unique(ns):
             idx = np.flatnonzero(ns == n)
             sh = np.arange(int(n) - 1, -1, -1, dtype=np.uint64)
             mat = ((xs[idx][:, None] >> sh[None, :]) & np.uint64(1)).astype(np.int32)
             for row, i in enumerate(idx):
                 bits[i] = mat[row]
-        names = [f[0] for f in QbResult._fields_]
-        return [_row_dict(dict(zip(names, row)), bits[i]) for i, row in enumerate(arr.tolist())]
+        c = {name: arr[name].tolist() for name, _ in QbResult._fields_}
+        forms = [FORM_NAMES.get(f, str(f)) for f in c["form_used"]]
+        return [{
+            "found": bool(c["found"][i]), "best_X_int": c["best_x"][i], "best_X": bits[i],
+            "best_E": c["best_e"][i], "best_E_int": c["best_e_int"][i], "order_key": c["order_key"][i],
+            "pass1_min": c["pass1_min"][i], "err_bound": c["err_bound"][i], "states": c["states"][i],
+            "candidate_records": c["candidate_records"][i], "form": forms[i], "is_integer": bool(c["is_integer"][i]),
+            "pass1_ms": c["pass1_ms"][i], "pass2_ms": c["pass2_ms"][i], "kernels": c["kernels"][i],
+            "kernel_ms": c["kernel_ms"][i], "h2d_bytes": c["h2d_bytes"][i], "d2h_bytes": c["d2h_bytes"][i],
+        } for i in range(count)]
 
     def prefix_minima(self, Q: np.ndarray, prefix_bits: int = -1) -> np.ndarray:
         """Per-prefix minimum energies in QBF's Gray visiting order (qb_prefix_minima)."""
@@ -270,30 +289,6 @@ def result_dict(r: QbResult, n: int) -> dict:
         "kernel_ms": float(r.kernel_ms),
         "h2d_bytes": int(r.h2d_bytes),
         "d2h_bytes": int(r.d2h_bytes),
-    }
-
-
-def _row_dict(f: dict, bits: np.ndarray) -> dict:
-    """result_dict of one row of a structured array of qb_result (field name -> value)."""
-    return {
-        "found": bool(f["found"]),
-        "best_X_int": int(f["best_x"]),
-        "best_X": bits,
-        "best_E": float(f["best_e"]),
-        "best_E_int": int(f["best_e_int"]),
-        "order_key": int(f["order_key"]),
-        "pass1_min": float(f["pass1_min"]),
-        "err_bound": float(f["err_bound"]),
-        "states": int(f["states"]),
-        "candidate_records": int(f["candidate_records"]),
-        "form": FORM_NAMES.get(int(f["form_used"]), str(f["form_used"])),
-        "is_integer": bool(f["is_integer"]),
-        "pass1_ms": float(f["pass1_ms"]),
-        "pass2_ms": float(f["pass2_ms"]),
-        "kernels": int(f["kernels"]),
-        "kernel_ms": float(f["kernel_ms"]),
-        "h2d_bytes": int(f["h2d_bytes"]),
-        "d2h_bytes": int(f["d2h_bytes"]),
     }
 
 

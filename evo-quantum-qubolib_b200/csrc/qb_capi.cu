@@ -100,7 +100,7 @@ struct qb_handle_s {
   DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
   DevBuf bat[14];  // qb_solve_batch: W, insts, gtab items, unit items, selection ids, cands, out, G tables,
                    // records, minima, scaled W, tensor-core items, item ranges, error word
-  HostBuf hW, hmisc, hout;
+  HostBuf hW, hmisc, hout, hbat;  // hbat: qb_solve_batch's packed W matrices (pinned)
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // 4, 5: main kernel
   int64_t h2d = 0, d2h = 0;  // bytes copied by the current call
   float kernel_ms = 0.f;
@@ -150,6 +150,34 @@ double load_elem(const unsigned char* p, int dt) {
     case QB_I32: { int32_t v; memcpy(&v, p, 4); return v; }
     default: { int64_t v; memcpy(&v, p, 8); return (double)v; }
   }
+}
+
+// Q in host memory (any dtype) -> W (n x n doubles, written to Wout) and sum |Q_ij|, without
+// intermediate copies (the batched search packs thousands of these).
+int load_host_problem_into(const qb_problem* p, double* Wout, double* abs_sum, bool* is_int) {
+  const int n = p->n;
+  const int es = dtype_size(p->dtype);
+  const unsigned char* src = static_cast<const unsigned char*>(p->q);
+  const size_t ld = (size_t)p->ldq * es;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) {
+    for (int j = i; j < n; ++j) {
+      const double a = load_elem(src + i * ld + (size_t)j * es, p->dtype);
+      if (i == j) {
+        if (!std::isfinite(a)) return QB_EINVAL;
+        s += std::fabs(a);
+        Wout[(size_t)i * n + i] = a;
+      } else {
+        const double b = load_elem(src + j * ld + (size_t)i * es, p->dtype);
+        if (!std::isfinite(a) || !std::isfinite(b)) return QB_EINVAL;
+        s += std::fabs(a) + std::fabs(b);
+        Wout[(size_t)i * n + j] = Wout[(size_t)j * n + i] = a + b;
+      }
+    }
+  }
+  *abs_sum = s;
+  *is_int = p->dtype >= QB_I8;
+  return QB_OK;
 }
 
 // Q (any dtype, host or device) -> W (n x n doubles) and sum |Q_ij|.
@@ -415,6 +443,7 @@ int qb_handle_destroy(qb_handle* h) {
   h->hW.release();
   h->hmisc.release();
   h->hout.release();
+  h->hbat.release();
   for (auto& ev : h->ev)
     if (ev) cudaEventDestroy(ev);
   if (h->own) cudaStreamDestroy(h->own);
@@ -940,11 +969,16 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   const int m = (int)ids.size();
   if (!m) return QB_OK;
   std::vector<qb::BatchInst> insts(m);
-  std::vector<double> Wall;
+  // every problem's W, then the tensor-core problems' scaled W, packed in pinned memory
+  uint64_t w_total = 0;
+  for (int j = 0; j < m; ++j) w_total += (uint64_t)problems[ids[j]].n * problems[ids[j]].n;
+  QB_CUDA(h->hbat.ensure(2 * w_total * sizeof(double) + 64));
+  double* Wall = static_cast<double*>(h->hbat.p);
+  double* Wtc = Wall + w_total;
+  uint64_t w_used = 0, wtc_used = 0;
   std::vector<qb::BatchItem> gitems, uitems;
   std::vector<uint32_t> gray_ids;  // problems with a selection step (Gray and tensor-core forms)
   std::vector<qb::BatchCand> pre;
-  std::vector<double> Wtc;                    // scaled W of the tensor-core problems
   std::vector<std::pair<int, uint64_t>> tcs;  // (problem, offset in Wtc)
   uint64_t gtab_total = 0, rec_total = 0;
   size_t sm_gtab = 0, sm_gray = 0, sm_exact = 0;
@@ -953,13 +987,20 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   const bool tc_allowed = o->form == QB_FORM_AUTO || o->form == QB_FORM_TC;
   for (int j = 0; j < m; ++j) {
     const qb_problem* p = &problems[ids[j]];
-    std::vector<double> W;
+    const int n = p->n;
+    double* W = Wall + w_used;
     double abs_sum = 0.0;
     bool is_int = false;
-    int rc = load_problem(h, p, W, &abs_sum, &is_int);
+    int rc;
+    if (p->q_on_device) {
+      std::vector<double> Wv;
+      rc = load_problem(h, p, Wv, &abs_sum, &is_int);
+      if (!rc) memcpy(W, Wv.data(), Wv.size() * sizeof(double));
+    } else {
+      rc = load_host_problem_into(p, W, &abs_sum, &is_int);
+    }
     if (rc) return rc;
     if (abs_sum >= kTwo53) return QB_ERANGE;
-    const int n = p->n;
     qb::BatchInst& I = insts[j];
     memset(&I, 0, sizeof(I));
     I.n = n;
@@ -968,8 +1009,8 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     I.A = o->prefix_bits < 0 ? n - std::min(n, 20) : o->prefix_bits;
     if (I.A > n) return QB_EINVAL;
     I.B = n - I.A;
-    I.w_off = Wall.size();
-    Wall.insert(Wall.end(), W.begin(), W.end());
+    I.w_off = w_used;
+    w_used += (uint64_t)n * n;
     int free_bits;
     if (n >= kBatchTcMinN && tc_allowed && qb::tc_supported(n)) {
       qb::TcPlan tp;
@@ -982,8 +1023,9 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
       I.eps = tp.eps;
       I.rec_off = rec_total;
       rec_total += I.nrec;
-      tcs.emplace_back(j, (uint64_t)Wtc.size());
-      for (double v : W) Wtc.push_back(v * tp.scale);
+      tcs.emplace_back(j, wtc_used);
+      for (uint64_t e = 0; e < (uint64_t)n * n; ++e) Wtc[wtc_used + e] = W[e] * tp.scale;
+      wtc_used += (uint64_t)n * n;
       gray_ids.push_back((uint32_t)j);
       n_tc_max = std::max(n_tc_max, n);
       free_bits = I.gl + 12;
@@ -1024,7 +1066,9 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   // device buffers
   DevBuf* B = h->bat;
   int rc;
-  if ((rc = upload_vec(h, B[0], Wall))) return rc;
+  QB_CUDA(B[0].ensure(std::max<uint64_t>(w_used, 2) * sizeof(double)));
+  QB_CUDA(cudaMemcpyAsync(B[0].p, Wall, w_used * sizeof(double), cudaMemcpyHostToDevice, h->st));
+  h->h2d += (int64_t)(w_used * sizeof(double));
   if ((rc = upload_vec(h, B[1], insts))) return rc;
   if ((rc = upload_vec(h, B[2], gitems))) return rc;
   if ((rc = upload_vec(h, B[3], uitems))) return rc;
@@ -1099,12 +1143,13 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     }
     if (first.back() != (uint32_t)items.size()) first.push_back((uint32_t)items.size());
     // device addresses
-    QB_CUDA(B[10].ensure(std::max<size_t>(Wtc.size(), 1) * sizeof(double)));
+    QB_CUDA(B[10].ensure(std::max<uint64_t>(wtc_used, 2) * sizeof(double)));
     for (size_t k = 0; k < items.size(); ++k) {
       items[k].W = static_cast<const double*>(B[10].p) + offs[k].first;
       items[k].rec = static_cast<float*>(B[8].p) + offs[k].second;
     }
-    if ((rc = upload_vec(h, B[10], Wtc))) return rc;
+    QB_CUDA(cudaMemcpyAsync(B[10].p, Wtc, wtc_used * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    h->h2d += (int64_t)(wtc_used * sizeof(double));
     if ((rc = upload_vec(h, B[11], items))) return rc;
     if ((rc = upload_vec(h, B[12], first))) return rc;
     QB_CUDA(B[13].ensure(16));
