@@ -18,11 +18,13 @@
 // the two C columns of B change.  The epilogue reads the accumulators (tcgen05.ld), takes
 // row minima with 3-input fp32 min and adds R_t(y).
 //
-// Measured on B200 (sm_100a): one N=256 MMA per 32768 states, consumed through
-// tcgen05.commit / mbarrier, costs about 450 cycles of pipeline round trip, and smaller N
-// does not shorten it, so tiles use the largest N; the TMEM holds two 256-column
-// accumulator stages.  The fp32 min pipe (about 128 values per clock per SM, shared with
-// fp32 adds) bounds the epilogue at half the MMA rate.
+// Measured on B200 (sm_100a): back to back, an M=128 N=256 K=16 MMA takes 128 cycles; a
+// one-way mbarrier signal between two warps (arrive -> try_wait returns) about 270 cycles.
+// A tile's accumulator stage is busy for MMA + commit signal + epilogue loads + release
+// signal + the MMA thread's reaction, so with the two 256-column stages the TMEM holds,
+// throughput is set by that round trip; smaller N does not shorten it, so tiles use the
+// largest N.  The fp32 min pipe (about 128 values per clock per SM, shared with fp32 adds)
+// bounds the epilogue at half the MMA rate.
 //
 // Roles (one persistent CTA per SM, 640 threads):
 //   warp 0      tile walk: 32 tiles per step, one per lane.  t = (t_hi, t_lo) with t_lo the
@@ -156,23 +158,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// try_wait with a suspend-time hint: the warp sleeps in hardware until the phase completes
-// (or the hint, in ns, runs out) instead of spinning on shared memory
-__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(b)), "r"(parity), "r"(1000000u)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait: false on timeout (or when another role already gave up)
+// bounded wait: false on timeout (or when another role already gave up).  try_wait suspends
+// the warp in hardware until the phase completes or a system-dependent time limit runs out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
   if (mbar_try_wait(b, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (;;) {
-    if (mbar_try_wait_sleep(b, parity)) return true;
+    if (mbar_try_wait(b, parity)) return true;
     if (*abort_flag) return false;
     if (globaltimer_ns() - t0 > kTcWaitLimitNs) return false;
   }
@@ -533,28 +525,36 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       }
     } else if (warp == 1) {
       // ---------------------------------------------------------- MMA issue
+      // Unrolled over the 8 B stages: the CTA-wide tile counter starts every item at a
+      // multiple of 8 and an item has a multiple of 32 tiles, so the stage of each unrolled
+      // step and its accumulator-barrier parity are constants.  The issuing thread shares its
+      // scheduler with four epilogue warps; a short per-tile instruction chain keeps MMA j + 2
+      // close behind the release of tile j.
       if (lane == 0) {
         const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
+        const uint64_t bdesc0 = umma_desc(smem_u32(Bsm), 128, 256);
         const uint32_t nt32 = (uint32_t)ntiles;
-        uint32_t issued = 0;
-        for (uint32_t jl = 0; jl < nt32 && ok; ++jl) {
-          const uint32_t j = jbase + jl;
-          const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-          const uint32_t as = j & 1u;
-          ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag) &&
-               mbar_wait(&acc_empty[as], ((j >> 1) & 1u) ^ 1u, abort_flag);
-          if (!ok) break;
-          tc_fence_after();
-          // every epilogue warp has released tile j-2 (it read that tile's row terms before its
-          // release, and MMA j-2 completed before the tile could be read): its B stage is free
-          if (j >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(j - kTcStages) & (uint32_t)(kTcBStages - 1)]);
-          const uint64_t bdesc = umma_desc(smem_u32(Bsm + bs * kTcN * 32), 128, 256);
-          tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc);
-          tc_commit(&acc_full[as]);  // one commit per MMA
-          issued = jl + 1;
+        for (uint32_t jl0 = 0; jl0 < nt32 && ok; jl0 += kTcBStages) {
+          const uint32_t j0 = jbase + jl0;
+          const uint32_t pb = (j0 >> 3) & 1u;  // b_full parity of the 8 tiles
+#pragma unroll
+          for (int k = 0; k < kTcBStages; ++k) {
+            const uint32_t as = (uint32_t)k & 1u;
+            // tile j0 + k: its B stage is full and tile j0 + k - 2 has left accumulator stage as
+            ok = mbar_wait(&b_full[k], pb, abort_flag) &&
+                 mbar_wait(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
+            if (!ok) break;
+            tc_fence_after();
+            // every epilogue warp has released tile j-2 (it read that tile's row terms before its
+            // release, and MMA j-2 completed before the tile could be read): its B stage is free
+            if (j0 + (uint32_t)k >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(k + kTcBStages - kTcStages) % kTcBStages]);
+            // B stage k starts k * 8 KB after stage 0 (descriptor address field in 16-byte units)
+            tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc0 + (uint64_t)(k * (kTcN * 32 / 16)));
+            tc_commit(&acc_full[as]);  // one commit per MMA
+          }
         }
-        if (issued) {  // the last MMA completes before the item's operands can change
-          const uint32_t j = jbase + issued - 1;
+        if (ok && nt32) {  // the last MMA completes before the item's operands can change
+          const uint32_t j = jbase + nt32 - 1;
           mbar_wait(&acc_full[j & 1u], (j >> 1) & 1u, abort_flag);
         }
       }
