@@ -38,6 +38,9 @@ struct GrayParams {
   float* rec;         // record minima; rec[0] holds record (unit_begin << (gubits + 3))
 };
 
+// trailing zeros of 1 <= l < 32 (folds to a constant for an unrolled l)
+__host__ __device__ constexpr int ctz5(int l) { return (l & 1) ? 0 : (l & 2) ? 1 : (l & 4) ? 2 : (l & 8) ? 3 : 4; }
+
 // per-state error bound of the fp32 path (see the header comment)
 inline double gray_error_bound(double abs_sum) { return 300.0 * abs_sum * 5.9604644775390625e-08; }
 
@@ -163,6 +166,9 @@ __device__ __forceinline__ void gray_unit_body(const GrayParams& g, uint64_t uni
     alpha_f[k * kGrayThreads + t] = (float)s;
   }
   __syncthreads();
+  float alo[5];  // fp32 cross terms of the 5 low prefix bits (variables a-1-k), fixed per thread
+#pragma unroll
+  for (int k = 0; k < 5; ++k) alo[k] = alpha_f[(a - 1 - k) * kGrayThreads + t];
   float2 e2[16];
 #pragma unroll
   for (int c2 = 0; c2 < 16; ++c2) {
@@ -206,43 +212,59 @@ __device__ __forceinline__ void gray_unit_body(const GrayParams& g, uint64_t uni
       for (int q = 0; q < 4; ++q) nxt[q] = src[t + q * kGrayThreads];
     }
     const float* cur = gbuf + (blk & 1) * kGrayStage * 32;
-#pragma unroll 2
-    for (int jj = 0; jj < kGrayStage; ++jj) {
-      const uint32_t i = ib + jj;
-      if (jj) {
-        const int kb = __ffs(i) - 1;
+    // 4 aligned groups of 32 steps.  Inside a group the flipped prefix bit of step l > 0 is
+    // kb = ctz(l) and its new state is !bit(kb + 1) of the step index: both constants of
+    // the unrolled step for kb < 4; for kb = 4 bit 5 is the group's parity (the block
+    // starts at a multiple of 128).  A group's first step flips a bit >= 5 (general code).
+    for (int grp = 0; grp < kGrayStage / 32; ++grp) {
+      const uint32_t ig = ib + (uint32_t)grp * 32u;
+      if (grp) {
+        const int kb = __ffs(ig) - 1;
         const int var = a - 1 - kb;
         const float al = alpha_f[var * kGrayThreads + t];
-        A = ((i ^ (i >> 1)) >> kb) & 1 ? A + al : A - al;
+        A = ((ig ^ (ig >> 1)) >> kb) & 1 ? A + al : A - al;
       }
-      const float4* row = reinterpret_cast<const float4*>(cur + jj * 32);
-      float2 v[16];
+      const float a4 = (grp & 1) ? -alo[4] : alo[4];
+      const float* crow = cur + grp * 32 * 32;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        float4 gg = row[q];
-        v[2 * q] = fadd2(e2[2 * q], make_float2(gg.x, gg.y));
-        v[2 * q + 1] = fadd2(e2[2 * q + 1], make_float2(gg.z, gg.w));
+      for (int l = 0; l < 32; ++l) {
+        if (l) {
+          const int kb = ctz5(l);
+          if (kb < 4)
+            A = ((l >> (kb + 1)) & 1) ? A - alo[kb] : A + alo[kb];
+          else
+            A += a4;
+        }
+        const float4* row = reinterpret_cast<const float4*>(crow + l * 32);
+        float2 v[16];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          float4 gg = row[q];
+          v[2 * q] = fadd2(e2[2 * q], make_float2(gg.x, gg.y));
+          v[2 * q + 1] = fadd2(e2[2 * q + 1], make_float2(gg.z, gg.w));
+        }
+        float m0 = fmin3(v[0].x, v[0].y, v[1].x);
+        float m1 = fmin3(v[1].y, v[2].x, v[2].y);
+        float m2 = fmin3(v[3].x, v[3].y, v[4].x);
+        float m3 = fmin3(v[4].y, v[5].x, v[5].y);
+        float m4 = fmin3(v[6].x, v[6].y, v[7].x);
+        float m5 = fmin3(v[7].y, v[8].x, v[8].y);
+        float m6 = fmin3(v[9].x, v[9].y, v[10].x);
+        float m7 = fmin3(v[10].y, v[11].x, v[11].y);
+        float m8 = fmin3(v[12].x, v[12].y, v[13].x);
+        float m9 = fmin3(v[13].y, v[14].x, v[14].y);
+        float n0 = fmin3(m0, m1, m2);
+        float n1 = fmin3(m3, m4, m5);
+        float n2 = fmin3(m6, m7, m8);
+        float n3 = fmin3(m9, v[15].x, v[15].y);
+        float mm = fmin3(n0, n1, fminf(n2, n3));
+        rmin = fminf(rmin, mm + A);
       }
-      float m0 = fmin3(v[0].x, v[0].y, v[1].x);
-      float m1 = fmin3(v[1].y, v[2].x, v[2].y);
-      float m2 = fmin3(v[3].x, v[3].y, v[4].x);
-      float m3 = fmin3(v[4].y, v[5].x, v[5].y);
-      float m4 = fmin3(v[6].x, v[6].y, v[7].x);
-      float m5 = fmin3(v[7].y, v[8].x, v[8].y);
-      float m6 = fmin3(v[9].x, v[9].y, v[10].x);
-      float m7 = fmin3(v[10].y, v[11].x, v[11].y);
-      float m8 = fmin3(v[12].x, v[12].y, v[13].x);
-      float m9 = fmin3(v[13].y, v[14].x, v[14].y);
-      float n0 = fmin3(m0, m1, m2);
-      float n1 = fmin3(m3, m4, m5);
-      float n2 = fmin3(m6, m7, m8);
-      float n3 = fmin3(m9, v[15].x, v[15].y);
-      float mm = fmin3(n0, n1, fminf(n2, n3));
-      rmin = fminf(rmin, mm + A);
-      if ((i & rmask) == rmask) {  // end of an aligned record group (uniform across the CTA)
+      const uint32_t ilast = ig + 31u;
+      if ((ilast & rmask) == rmask) {  // end of an aligned record group (sbits >= 5; uniform)
         float wmin = warp_min_f(rmin);
         if (lane == 0) {
-          const uint64_t gi = (uint64_t)((i - i0) >> g.sbits);
+          const uint64_t gi = (uint64_t)((ilast - i0) >> g.sbits);
           g.rec[rec_unit_base | (gi << 3) | (uint64_t)warp] = wmin;
         }
         rmin = inf;
