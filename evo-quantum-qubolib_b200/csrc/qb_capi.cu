@@ -827,7 +827,7 @@ int qbf1_wrap_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_r
                             (size_t)A * A * sizeof(int), h->st>>>(dQ, n, A, AA);
   const uint64_t nchunks = std::min<uint64_t>(64, std::max<uint64_t>(4, steps));
   const uint64_t chunk_len = (steps + nchunks - 1) / nchunks;
-  const size_t sm = (size_t)A * 1024 * sizeof(short);
+  const size_t sm = qb::qbf1w_search_smem(A);
   QB_CUDA(cudaFuncSetAttribute(qb::qbf1w_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   QB_CUDA(cudaEventRecord(h->ev[4], h->st));
   qb::qbf1w_search_kernel<<<dim3(qb::kQbf1Threads / 64, (unsigned)(nchunks / 4)), 256, sm, h->st>>>(

@@ -268,7 +268,7 @@ def qbf1_int16_numpy(Q) -> dict:
       earliest step; the initial best is the min over the columns at prefix 0;
       pack_results (:253-289): lowest thread with the smallest int16 best; its prefix's
       int16 row argmin (first) gives the suffix; best_E is the thread's int16 value.
-    n in [19, 26] (vectorised over the 16384 threads)."""
+    n in [19, 31] (vectorised over the 16384 threads; 2^(n-18) steps, about 2.5 s at n = 29)."""
     Q = np.asarray(Q)
     assert Q.dtype == np.int16
     n = Q.shape[0]

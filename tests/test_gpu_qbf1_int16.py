@@ -18,7 +18,9 @@ def _xint(sol):
     return bits_to_int("".join(map(str, sol.best_X)))
 
 
-@pytest.mark.parametrize("n,hi,seed", [(19, 100, 1), (20, 100, 2), (21, 3000, 3), (22, 30000, 4), (23, 900, 5)])
+# n < 29: chunks shorter than 32 steps (the per-step loop); n >= 29: aligned groups of 32 steps
+@pytest.mark.parametrize("n,hi,seed", [(19, 100, 1), (20, 100, 2), (21, 3000, 3), (22, 30000, 4), (23, 900, 5),
+                                       (29, 3000, 8), (30, 200, 9)])
 def test_int16_wrap_matches_restated_reference(cuda_ok, n, hi, seed):
     Q = np.random.default_rng(seed).integers(-hi, hi, (n, n)).astype(np.int16)
     ref = oracle.qbf1_int16_numpy(Q)
