@@ -377,6 +377,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     // variables: t bit k <-> n-16-k, y bit i <-> n-9-i, u bit j <-> n-1-j
 
     // ------------------------------------------------------------ per-item set-up
+    if (kItems && tid == 0) {  // read by the epilogue at record flushes (keeps them out of registers)
+      *reinterpret_cast<float**>(tc_smem + L.misc_off + 16) = rec;
+      *reinterpret_cast<float*>(tc_smem + L.misc_off + 24) = inv_scale;
+    }
     for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = I.W[i];
     // the item's records start at +inf (the epilogue folds into them with atomic minima)
     for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
@@ -632,7 +636,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       // of this warp's parity), counted down from the CTA's first block (aligned to 2^gl)
       const uint32_t nt32 = (uint32_t)ntiles;
       uint32_t rec_left = 1u << (gl - 1);
-      uint64_t Jrec = 0;
+      uint32_t Jrec = 0;  // records of this item (fewer than 2^31)
       for (uint32_t jl = sp; jl < nt32 && ok; jl += 2) {
         const uint32_t j = jbase + jl;  // CTA-wide tile counter (jbase is even)
         const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
@@ -663,9 +667,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         rmin = fminf(rmin, m + R);
         if (--rec_left == 0) {
           // both parities' warps of (column half, lane quarter) fold into one record
-          const float wm = warp_min_f(rmin) * inv;
+          // the multi-item kernel re-reads the item's record base and scale from shared memory
+          const float sc = kItems ? *reinterpret_cast<volatile float*>(tc_smem + L.misc_off + 24) : inv;
+          float* rb0 = kItems ? *reinterpret_cast<float* volatile*>(tc_smem + L.misc_off + 16) : rec;
+          const float wm = warp_min_f(rmin) * sc;
           if (lane == 0) {
-            float* dst = rec + ((Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+            float* dst = rb0 + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
             if (wm >= 0.f)
               atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
             else
