@@ -137,6 +137,10 @@ __host__ __device__ __forceinline__ float key2f(uint32_t k) {
 #endif
 }
 
+// trailing zeros of 1 <= l < 32 (folds to a constant for an unrolled l): the prefix bit
+// flipped by step l of an aligned group of 32 Gray steps
+__host__ __device__ constexpr int ctz5(int l) { return (l & 1) ? 0 : (l & 2) ? 1 : (l & 4) ? 2 : (l & 8) ? 3 : 4; }
+
 #ifdef __CUDACC__
 __device__ __forceinline__ uint64_t globaltimer_ns() {
   uint64_t t;

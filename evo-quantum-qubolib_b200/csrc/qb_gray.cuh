@@ -38,9 +38,6 @@ struct GrayParams {
   float* rec;         // record minima; rec[0] holds record (unit_begin << (gubits + 3))
 };
 
-// trailing zeros of 1 <= l < 32 (folds to a constant for an unrolled l)
-__host__ __device__ constexpr int ctz5(int l) { return (l & 1) ? 0 : (l & 2) ? 1 : (l & 4) ? 2 : (l & 8) ? 3 : 4; }
-
 // per-state error bound of the fp32 path (see the header comment)
 inline double gray_error_bound(double abs_sum) { return 300.0 * abs_sum * 5.9604644775390625e-08; }
 

@@ -78,9 +78,6 @@ __device__ __forceinline__ uint32_t min16x2(uint32_t x, uint32_t y) {
 }
 __device__ __forceinline__ uint32_t pack16(int lo, int hi) { return (uint32_t)(uint16_t)lo | ((uint32_t)(uint16_t)hi << 16); }
 
-// trailing zeros of 1 <= l < 32 (folds to a constant for an unrolled l)
-__host__ __device__ constexpr int qbf1_ctz5(int l) { return (l & 1) ? 0 : (l & 2) ? 1 : (l & 4) ? 2 : (l & 8) ? 3 : 4; }
-
 // shared memory of the search kernel: +ABBA and -ABBA rows of the block's 1024 columns,
 // two columns per 32-bit word
 inline size_t qbf1w_search_smem(int A) { return (size_t)2 * A * 512 * sizeof(uint32_t); }
@@ -170,7 +167,7 @@ __global__ void __launch_bounds__(256) qbf1w_search_kernel(int A, const short* _
           const bool on = (gray64(ig) >> kb) & 1;
           r = (on ? pos : neg) + (A - 1 - kb) * 512;
         } else {
-          const int kb = qbf1_ctz5(l);
+          const int kb = ctz5(l);
           const bool on = kb < 4 ? !((l >> (kb + 1)) & 1) : !odd;
           r = (on ? pos : neg) + (A - 1 - kb) * 512;
         }
