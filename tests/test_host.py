@@ -147,3 +147,27 @@ def test_config_generators_match_reference_inputs():
     np.testing.assert_array_equal(configs.maxcut_er(), dec_q(cfg["cfg4"]["Q"]))
     for b in cfg["cfg5_subset"]:
         np.testing.assert_array_equal(configs.batch_instance(b["index"], seed=1000), dec_q(b["Q"]))
+
+
+def test_gray_group_identities():
+    """The Gray-form and QB_F1 int16 kernels walk Gray steps in aligned groups of 32
+    with constants in place of a per-step bit scan.  The identities they rely on: for ig a
+    multiple of 32 and 0 <= l < 32, gray(ig + l) = gray(ig) ^ gray(l); step l > 0 flips bit
+    ctz(l), which turns on unless bit ctz(l) + 1 of the step index is set (bit 5 of ig when
+    ctz(l) = 4); and ctz5 in csrc/qb_common.cuh is ctz on 1..31."""
+    def gray(i):
+        return i ^ (i >> 1)
+
+    def ctz5(l):  # restated from csrc/qb_common.cuh
+        return 0 if l & 1 else 1 if l & 2 else 2 if l & 4 else 3 if l & 8 else 4
+
+    rng = np.random.default_rng(3)
+    for ig in [0, 32, 96, 4096] + [int(v) * 32 for v in rng.integers(0, 1 << 30, 200)]:
+        for l in range(32):
+            assert gray(ig + l) == gray(ig) ^ gray(l)
+            if l:
+                kb = ctz5(l)
+                assert kb == (l & -l).bit_length() - 1
+                turns_on = bool((gray(ig + l) >> kb) & 1)
+                predicted = not ((l >> (kb + 1)) & 1) if kb < 4 else not ((ig >> 5) & 1)
+                assert turns_on == predicted
