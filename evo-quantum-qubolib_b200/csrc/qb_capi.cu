@@ -1393,7 +1393,9 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
 //
 // Set-up: the first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (with that device current) and caches it; make that first call
-// before any stream capture.  All calls share the one array and every call overwrites it:
+// before any stream capture, and make it a complete, valid solve (20 <= n <= 36, finite Q)
+// so that it also launches every kernel the entry point uses: with CUDA's lazy module
+// loading the first launch of a kernel can load code and take device memory.  All calls share the one array and every call overwrites it:
 // calls whose work overlaps on the GPU (other streams, other threads) race and must be
 // serialised by the caller.
 // ---------------------------------------------------------------------------------------
@@ -1417,6 +1419,7 @@ struct NoAllocMisc {  // lives at the end of g_noalloc_scratch
   double threshold;
   uint32_t min_key;
   int cand_count;
+  int bad_input;  // Q held a NaN / infinity, or a fractional value with is_integer set
 };
 
 static_assert(sizeof(NoAllocMisc) <= kNoAllocMisc, "misc block");
@@ -1425,16 +1428,22 @@ static_assert(kNoAllocBytes == 16924928, "scratch size stated in include/qubo_b2
 std::mutex g_noalloc_lock;
 void* g_noalloc_addr[128] = {nullptr};
 
-__global__ void noalloc_prep_kernel(const double* __restrict__ Q, int n, double* __restrict__ W,
+// W from Q, sum |Q_ij|, and the input checks that qb_solve makes on the host: every entry
+// finite and, when the caller says Q is integer, integral (a fractional entry would make the
+// exact path's zero error band drop the true minimum)
+__global__ void noalloc_prep_kernel(const double* __restrict__ Q, int n, int is_int, double* __restrict__ W,
                                     NoAllocMisc* __restrict__ misc) {
   __shared__ double part[256];
   double s = 0.0;
+  int bad = 0;
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int i = e / n, j = e % n;
     const double q = Q[e];
+    if (!isfinite(q) || (is_int && q != trunc(q))) bad = 1;
     s += fabs(q);
     W[e] = (i == j) ? q : q + Q[j * n + i];
   }
+  bad = __syncthreads_or(bad);
   part[threadIdx.x] = s;
   __syncthreads();
   for (int off = blockDim.x / 2; off; off >>= 1) {
@@ -1445,6 +1454,7 @@ __global__ void noalloc_prep_kernel(const double* __restrict__ Q, int n, double*
     misc->abs_sum = part[0];
     misc->min_key = 0xffffffffu;
     misc->cand_count = 0;
+    misc->bad_input = bad;
   }
 }
 
@@ -1452,9 +1462,13 @@ __global__ void noalloc_threshold_kernel(NoAllocMisc* __restrict__ misc, int is_
   const double m = (double)qb::key2f(misc->min_key);
   const double S = misc->abs_sum;
   // the Gray form's per-state bound on |fp32 pass-1 value - exact energy| (300 ulp of S)
-  const double eps = (is_int && S < 16777216.0) ? 0.0 : 300.0 * S * 5.9604644775390625e-08;
+  const bool exact_int = is_int && S < 16777216.0;
+  const double eps = exact_int ? 0.0 : 300.0 * S * 5.9604644775390625e-08;
   double thr = m + 2.0 * eps;
   if (eps > 0.0) thr += fabs(thr) * 1e-12;
+  // nothing to re-walk when the answer is already known: rejected input, or exact integer
+  // arithmetic with no negative energy (X = 0, E = 0 is minimal and has the smallest key)
+  if (misc->bad_input || (exact_int && m >= 0.0)) thr = -__longlong_as_double(0x7ff0000000000000ll);
   misc->threshold = thr;
   misc->cand_count = 0;
 }
@@ -1462,6 +1476,7 @@ __global__ void noalloc_threshold_kernel(NoAllocMisc* __restrict__ misc, int is_
 __global__ void noalloc_select_kernel(const float* __restrict__ rec, int64_t count, const NoAllocMisc* misc,
                                       uint64_t* __restrict__ cand, int* __restrict__ cand_count, int cap) {
   const double thr = misc->threshold;
+  if (thr == -__longlong_as_double(0x7ff0000000000000ll)) return;  // nothing to select
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
     if ((double)rec[i] <= thr) {
@@ -1492,7 +1507,12 @@ __global__ void noalloc_final_kernel(const qb::ExactOut* __restrict__ eo, const 
   if (threadIdx.x == 0) {
     const double pmin = (double)qb::key2f(misc->min_key);
     const bool exact_int = is_int && misc->abs_sum < 16777216.0;
-    if (is_int && misc->abs_sum >= 9007199254740992.0) {  // sum |Q_ij| >= 2^53: FP64 not exact
+    if (misc->bad_input) {
+      out->best_e = 0.0;
+      out->best_x = 0ull;
+      out->order_key = 0ull;
+      out->status = QB_EINVAL;
+    } else if (is_int && misc->abs_sum >= 9007199254740992.0) {  // sum |Q_ij| >= 2^53: FP64 not exact
       out->best_e = 0.0;
       out->best_x = 0ull;
       out->order_key = 0ull;
@@ -1552,7 +1572,7 @@ int noalloc_run(int device, const double* q_dev, int n, int is_integer, int pref
   int sms = 0;
   QB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   const qb::ProblemDev pd{n, W};
-  noalloc_prep_kernel<<<1, 256, 0, st>>>(q_dev, n, W, misc);
+  noalloc_prep_kernel<<<1, 256, 0, st>>>(q_dev, n, is_integer ? 1 : 0, W, misc);
   const size_t sm0 = qb::gray_gtab_smem(n, a);
   QB_CUDA(cudaFuncSetAttribute(qb::gray_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm0));
   qb::gray_gtab_kernel<<<(unsigned)std::min<uint64_t>((1ull << a) / 8 + 1, (uint64_t)sms * 4), 256, sm0, st>>>(pd, a, b, gtab);

@@ -177,7 +177,9 @@ typedef struct qb_noalloc_result {
   double best_e;        /* E(best_x) in FP64 (exact for integer Q) */
   uint64_t best_x;      /* MSB-first state integer */
   uint64_t order_key;   /* QB_TIE_QBF key of best_x */
-  int32_t status;       /* QB_OK, or QB_EOVERFLOW when more candidate records than fit */
+  int32_t status;       /* QB_OK; QB_EOVERFLOW when more candidate records than fit;
+                           QB_EINVAL when Q holds a NaN or infinity, or a fractional entry
+                           with is_integer set; QB_ERANGE (see below) */
   int32_t candidates;   /* candidate records found by the selection */
 } qb_noalloc_result;
 
@@ -197,8 +199,11 @@ typedef struct qb_noalloc_result {
  * up to 4096 candidate records (out_dev->status = QB_EOVERFLOW beyond); integer Q needs
  * sum |Q_ij| < 2^53 (out_dev->status = QB_ERANGE otherwise).
  * The first call on a device resolves the array's address (cudaGetSymbolAddress with that
- * device current): make it before any stream capture.  Every call reuses the same array,
- * so calls that overlap on the GPU race; serialise them. */
+ * device current): make it before any stream capture, and make it a complete, valid solve
+ * (20 <= n <= 36, finite Q), not an early error return, so that it also launches every kernel
+ * the entry point uses once (with CUDA's lazy module loading a kernel's first launch can load
+ * code and take device memory) before capture begins or a memory budget is fixed.  Every
+ * call reuses the same array, so calls that overlap on the GPU race; serialise them. */
 int qb_solve_noalloc(int device, const double* q_dev, int32_t n, int32_t is_integer, int32_t prefix_bits,
                      qb_noalloc_result* out_dev, void* stream);
 

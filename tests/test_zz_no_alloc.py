@@ -1,14 +1,18 @@
-"""qb_solve_noalloc (the entry point that allocates nothing) against qb_solve.
+"""qb_solve_noalloc (the entry point that allocates nothing) against qb_solve and the oracle.
 
 Q and the result live in device memory owned by the caller (torch tensors here); the call
 goes through the C ABI with ctypes.  Each case runs two different problems back to back
-and compares both with qb_solve's Gray form on the same inputs.
+and compares both with qb_solve's Gray form on the same inputs and with the oracle (the C
+restatement of the reference's QBF loop): bit-exact for integer Q, the FP64 argmin with the
+energy within 1e-9 relative for float Q.  The status cases cover rejected input (NaN,
+fractional entries with is_integer set), too many candidate records and the 2^53 range.
 """
 import ctypes
 
 import numpy as np
 import pytest
 
+import oracle
 from qubo_b200 import _lib
 
 pytestmark = pytest.mark.gpu
@@ -66,6 +70,8 @@ def test_integer_two_calls_match_qb_solve(torch_cuda, n):
         assert r.best_e == ref["best_E"]  # integer energies: exact
         assert r.best_x == ref["best_X_int"]
         assert r.order_key == ref["order_key"]
+        orc = oracle.qbf_port(Q)
+        assert (r.best_x, r.best_e) == (orc["best_X_int"], orc["best_E"])
 
 
 @pytest.mark.parametrize("n", [22, 31])
@@ -81,6 +87,9 @@ def test_float_two_calls_match_qb_solve(torch_cuda, n):
         # both are FP64 re-evaluations of the same state: tolerance 1e-9 relative
         assert abs(r.best_e - ref["best_E"]) <= 1e-9 * max(1.0, abs(ref["best_E"]))
         assert r.best_x == ref["best_X_int"]
+        orc = oracle.qbf_port(Q)
+        assert r.best_x == orc["best_X_int"]
+        assert abs(r.best_e - orc["best_E"]) <= 1e-9 * max(1.0, abs(orc["best_E"]))
 
 
 def test_prefix_bits_and_repeat(torch_cuda):
@@ -95,6 +104,8 @@ def test_prefix_bits_and_repeat(torch_cuda):
         r = _read(torch, out)
         assert r.status == 0
         assert (r.best_e, r.best_x, r.order_key) == (ref["best_E"], ref["best_X_int"], ref["order_key"])
+    orc = oracle.qbf_port(Q, A=9)
+    assert (r.best_x, r.best_e) == (orc["best_X_int"], orc["best_E"])
 
 
 def test_no_device_memory_taken_after_setup(torch_cuda):
@@ -121,3 +132,45 @@ def test_sizes_outside_the_scratch_are_rejected(torch_cuda):
         rc, _, _ = _noalloc(torch, np.zeros((n, n)), True)
         assert rc == _lib.QB_ETOOBIG
     assert "no-allocation" in _lib.strerror(_lib.QB_ETOOBIG)
+
+
+def _status(torch, Q, is_integer):
+    rc, _, out = _noalloc(torch, Q, is_integer)
+    assert rc == 0  # the problem is queued; its verdict is in the device result
+    return _read(torch, out)
+
+
+def test_rejected_input(torch_cuda):
+    """NaN / infinity anywhere, or a fractional entry when the caller says Q is integer."""
+    torch = torch_cuda
+    base = _int_problem(24, 31).astype(np.float64)
+    for bad in (np.nan, np.inf, -np.inf):
+        Q = base.copy()
+        Q[3, 17] = bad
+        for is_int in (True, False):
+            assert _status(torch, Q, is_int).status == _lib.QB_EINVAL
+    Q = base.copy()
+    Q[5, 5] = 0.5
+    assert _status(torch, Q, True).status == _lib.QB_EINVAL
+    r = _status(torch, Q, False)  # the same matrix as float input is fine
+    orc = oracle.qbf_port(Q)
+    assert r.status == 0 and r.best_x == orc["best_X_int"]
+    assert abs(r.best_e - orc["best_E"]) <= 1e-9 * max(1.0, abs(orc["best_E"]))
+
+
+def test_too_many_candidates(torch_cuda):
+    """Float Q = 0: every record ties with the minimum, far more than the 4096 that fit."""
+    r = _status(torch_cuda, np.zeros((24, 24)), False)
+    assert r.status == _lib.QB_EOVERFLOW and r.candidates > 4096
+
+
+def test_integer_range_limit(torch_cuda):
+    Q = np.zeros((22, 22))
+    Q[0, 0] = -2.0 ** 53
+    assert _status(torch_cuda, Q, True).status == _lib.QB_ERANGE
+
+
+def test_zero_answer_needs_no_candidates(torch_cuda):
+    """Exact integer Q with no negative energy: X = 0 is the answer and nothing is re-walked."""
+    r = _status(torch_cuda, np.ones((26, 26)), True)
+    assert (r.status, r.best_x, r.best_e, r.order_key, r.candidates) == (0, 0, 0.0, 0, 0)
