@@ -1,5 +1,5 @@
-"""The ``energy_arr`` metric of ``use_metrics``: minimum energy per prefix, in the order the
-reference's prefix loop visits the prefixes.
+"""The ``energy_arr`` and ``time_arr`` metrics of ``use_metrics``, one entry per prefix in
+the order the reference's prefix loop visits the prefixes.
 
 QBF records one value per Gray step of its prefix loop: the smallest energy over all
 suffixes of that prefix (src/qubo_lib/solvers/qbf.py:395-412, returned as
@@ -7,12 +7,20 @@ suffixes of that prefix (src/qubo_lib/solvers/qbf.py:395-412, returned as
 each shifted by the task's prefix_E (src/qubo_lib/solvers/parallel.py:250-270).  Here the
 values come from the library's exact per-prefix kernel (qb_prefix_minima); they are exact
 FP64 sums, where the reference's float path carries fp32 accumulation drift.
+
+``time_arr`` in the reference holds the duration of each epoch of the prefix loop, one per
+prefix (PerformanceTimer picks labelled 'epoch', src/qubo_lib/solvers/qbf.py:362-365).  The
+GPU search has no per-prefix epochs: all prefixes of a solve are searched at once by one
+kernel, and every prefix covers the same number of states.  So each of the 2^A entries is
+an equal share of the solve's device time (pass 1 + pass 2), and the entries sum to it.
 """
 from __future__ import annotations
 
 import numpy as np
 
 from . import _lib
+
+MAX_PREFIX_BITS = 26  # 2^26 entries (512 MiB of float64): the limit of qb_prefix_minima too
 
 
 def _grayrank(g: np.ndarray) -> np.ndarray:
@@ -41,3 +49,11 @@ def parallel_energy_arr(Q: np.ndarray, task_bits: int, prefix_bits: int, device:
     i = np.arange(1 << A, dtype=np.uint64)[None, :]
     v = (t << np.uint64(A)) | (i ^ (i >> np.uint64(1)))  # natural prefix value of (task t, Gray step i)
     return out[_grayrank(v).astype(np.int64)].reshape(-1)
+
+
+def even_time_arr(total_ms: float, prefix_bits: int) -> np.ndarray:
+    """QBF's time_arr for one solve: 2^prefix_bits equal shares of total_ms (float64, ms)."""
+    A = int(prefix_bits)
+    if A > MAX_PREFIX_BITS:
+        raise ValueError(f"time_arr needs 2^{A} entries; at most 2^{MAX_PREFIX_BITS} are kept")
+    return np.full(1 << A, float(total_ms) / float(1 << A), dtype=np.float64)

@@ -176,7 +176,8 @@ class QBF(SolverABC):
             from .metrics import per_prefix_minima
             metric_dict["energy_arr"] = per_prefix_minima(self.Q, self.A, self.device_index)
         if "time_arr" in use_metrics:
-            metric_dict["time_arr"] = np.array([res["pass1_ms"] + res["pass2_ms"]])
+            from .metrics import even_time_arr
+            metric_dict["time_arr"] = even_time_arr(res["pass1_ms"] + res["pass2_ms"], self.A)
         sol.metrics = [metric_dict]
         sol.solver_class = "QBF"
         sol.best_E = self.glob_E
@@ -267,20 +268,54 @@ def _parse_cuda(dev: str) -> int:
     raise ValueError(f"Unknown device name: {dev}")
 
 
-def _worker_main(device: int, Q: np.ndarray, opts: dict, shard_index: int, shard_count: int, inbox, outbox):
-    """One device's share of a multi-device Parallel search (spawned process)."""
+def reduce_exact(Q: np.ndarray, k: int, task: int):
+    """Task ``task`` of Parallel's bit fixing: the first k variables fixed to the MSB-first
+    bits of ``task``.  Returns (reduced Q, prefix_E) by ReducedProblem's rule
+    (src/qubo_lib/problems/reduced_problem.py:31-46), Q' = Q[k:, k:] +
+    diag(p (Q[:k, k:] + Q[k:, :k]^T)) and prefix_E = p^T Q[:k, :k] p, computed exactly (int64
+    for integer Q, float64 otherwise) where the reference keeps the problem's dtype, so that a
+    task's answer equals the same states' answer in the single-device search."""
+    wide = np.int64 if np.issubdtype(Q.dtype, np.integer) else np.float64
+    Qw = np.asarray(Q).astype(wide)
+    p = np.array([(task >> (k - 1 - i)) & 1 for i in range(k)], dtype=wide)
+    prefix_E = (p @ Qw[:k, :k] @ p).item()
+    Qr = Qw[k:, k:] + np.diag(p @ (Qw[:k, k:] + Qw[k:, :k].T))
+    return np.ascontiguousarray(Qr), prefix_E
+
+
+def _task_worker(worker_id: int, device: int, Q: np.ndarray, opts: dict, tasks, results):
+    """One worker of a multi-worker Parallel search (spawned process, the reference's
+    scheduler.worker, src/qubo_lib/solvers/scheduler.py:48-59): takes task ids from the
+    shared queue until it reads None, solves each task's reduced problem on its device and
+    reports ("res", task, worker_id, result) or ("err", task, worker_id, message)."""
     try:
         stream = _torch_stream(device)
         h = _lib.handle(device)
-        t0 = time.perf_counter()
-        lmin = h.solve_begin(Q, shard_index=shard_index, shard_count=shard_count, stream=stream, **opts)
-        outbox.put(("min", shard_index, lmin))
-        gmin = inbox.get()
-        res = h.solve_finish(gmin, Q.shape[0])
-        res["time_ms"] = (time.perf_counter() - t0) * 1000
-        outbox.put(("res", shard_index, res))
-    except Exception as e:  # noqa: BLE001 - reported to the parent like the reference's worker
-        outbox.put(("err", shard_index, f"{type(e).__name__}: {e}"))
+    except Exception as e:  # noqa: BLE001 - reported to the parent
+        results.put(("err", None, worker_id, f"{type(e).__name__}: {e}"))
+        return
+    k = int(opts["fixed_bits"])
+    wrap = bool(opts.get("int16_wrap", False))
+    solve_opts = {key: v for key, v in opts.items() if key not in ("fixed_bits", "int16_wrap")}
+    while True:
+        task = tasks.get()
+        if task is None:
+            break
+        try:
+            t0 = time.perf_counter()
+            if wrap:  # the reference's own ReducedProblem: int16 arithmetic, wrapping as it does
+                from .problems import Just_Q, ReducedProblem
+                rp = ReducedProblem(Just_Q(Q), np.array([(task >> (k - 1 - i)) & 1 for i in range(k)]))
+                Qr = rp.build_Q_matrix()
+                pe = int(rp.prefix_E)
+            else:
+                Qr, pe = reduce_exact(Q, k, task)
+            res = h.solve(Qr, stream=stream, fixed_bits=0, int16_wrap=wrap, **solve_opts)
+            res["prefix_E"] = pe
+            res["time_ms"] = (time.perf_counter() - t0) * 1000
+            results.put(("res", task, worker_id, res))
+        except Exception as e:  # noqa: BLE001 - reported to the parent like the reference's worker
+            results.put(("err", task, worker_id, f"{type(e).__name__}: {e}"))
 
 
 class Parallel(SolverABC):
@@ -331,6 +366,7 @@ class Parallel(SolverABC):
         t0 = time.perf_counter()
         Q = np.asarray(problem.build_Q_matrix(use_gpu=False))
         m = N - k
+        workers = [_parse_cuda(d) for d in self._devices]  # one worker per entry, repeats included
         if self._solver_class_name == "QBF":
             A_sub, _ = QBF.define_chunk_size(N=m, size_of=Q.dtype.itemsize, **kwargs)
             opts = dict(form=kwargs.get("form", "auto"), tie_rule="qbf", fixed_bits=k, prefix_bits=A_sub)
@@ -339,48 +375,83 @@ class Parallel(SolverABC):
                 raise TypeError("Q dtype only np.int16 supported yet")
             if m < 19:
                 raise ValueError(f"QB_F1 needs N - log2(splits_cnt) >= 19, got {m}")
-            if kwargs.get("int16_wrap", False):
+            wrap = bool(kwargs.get("int16_wrap", False))
+            if wrap and len(workers) == 1:
                 return self._solve_qbf1_int16(problem, Q, k, json_str, t0, kwargs)
             opts = dict(form=kwargs.get("form", "auto"), tie_rule="qb_f1", fixed_bits=k)
-        devs = sorted(set(_parse_cuda(d) for d in self._devices))
-        if len(devs) == 1:
-            stream = _torch_stream(devs[0])
-            res = _lib.handle(devs[0]).solve(Q, stream=stream, **opts)
-            results = [res]
-            res["time_ms"] = (time.perf_counter() - t0) * 1000
+            if wrap:
+                opts["int16_wrap"] = True
+        n_tasks = self._splits_cnt
+        is_f1 = self._solver_class_name == "QB_F1"
+        if len(workers) == 1:
+            # one worker: every task is a prefix tile of one GPU search; the task bits lead
+            # the search's order key, so ties between tasks go to the lowest task id
+            stream = _torch_stream(workers[0])
+            best = _lib.handle(workers[0]).solve(Q, stream=stream, **opts)
+            total_ms = (time.perf_counter() - t0) * 1000
+            best_E = int(best["best_E_int"]) if is_f1 else np.float64(best["best_E"])
+            best_X = best["best_X"]
+            # the tasks run interleaved inside one search of equal-sized shares: each task is
+            # logged with an equal share of the search time
+            logs = [dict(task_id=t, worker_id=0, device=self._devices[0], time_to_solve_ms=total_ms / n_tasks)
+                    for t in range(n_tasks)]
+            time_to_solve = total_ms
+            parts = [best]
+            task_ms = [total_ms / n_tasks] * n_tasks
         else:
-            results = self._run_workers(devs, Q, opts, timeout)
-        found = [r for r in results if r["found"]]
-        if not found:
-            raise RuntimeError("no worker reported a minimising state")
-        best = min(found, key=lambda r: (r["best_E"], r["order_key"]))
+            done = self._run_workers(workers, Q, opts, n_tasks, timeout)
+            pick = None
+            for task in range(n_tasks):  # task order, strict <: the lowest task id wins ties
+                _, r = done[task]
+                E = (int(r["best_E_int"]) + int(r["prefix_E"])) if (is_f1 or r["is_integer"]) else \
+                    float(r["best_E"]) + float(r["prefix_E"])
+                if pick is None or E < pick[0]:
+                    pick = (E, task, r)
+            E, task, best = pick
+            prefix = np.array([(task >> (k - 1 - i)) & 1 for i in range(k)], dtype=best["best_X"].dtype)
+            best_X = np.hstack([prefix, best["best_X"]])
+            if is_f1:
+                best_E = int(E)
+            elif best["is_integer"]:
+                best_E = np.float64(E)
+            else:  # FP64 energy of the full state, as the single-device search reports it
+                xf = best_X.astype(np.float64)
+                best_E = np.float64(xf @ Q.astype(np.float64) @ xf)
+            logs = [dict(task_id=t, worker_id=done[t][0], device=self._devices[done[t][0]],
+                         time_to_solve_ms=done[t][1]["time_ms"]) for t in range(n_tasks)]
+            per_worker = {}
+            for t in range(n_tasks):
+                per_worker[done[t][0]] = per_worker.get(done[t][0], 0.0) + done[t][1]["time_ms"]
+            time_to_solve = max(per_worker.values())  # the busiest worker, as the reference reports
+            parts = [done[t][1] for t in range(n_tasks)]
+            task_ms = [done[t][1]["time_ms"] for t in range(n_tasks)]
         sol = Solution(N=N, epochs_cnt=self._splits_cnt, samples_cnt=1, problem_instance_json=problem.to_json(),
                        solver_params_json=json_str)
         sol.ising_offset = None
         sol.solver_class = self._solver_class_name
-        best_E = int(best["best_E_int"]) if (self._solver_class_name == "QB_F1") else np.float64(best["best_E"])
         sol.best_E = best_E
         sol.energies = np.array([best_E])
-        sol.best_X = best["best_X"]
-        sol.state_vectors = StateVectors(wide_vector_matrix=best["best_X"].reshape(1, -1))
+        sol.best_X = best_X
+        sol.state_vectors = StateVectors(wide_vector_matrix=best_X.reshape(1, -1))
         metrics = {}
         use_metrics = kwargs.get("use_metrics", set())
         if use_metrics == "all":
             use_metrics = ALL_METRICS
-        if "energy_arr" in use_metrics and self._solver_class_name == "QBF":
-            from .metrics import parallel_energy_arr
-            metrics["energy_arr"] = parallel_energy_arr(Q, k, opts["prefix_bits"], devs[0])
+        if not is_f1:
+            if "energy_arr" in use_metrics:
+                from .metrics import parallel_energy_arr
+                metrics["energy_arr"] = parallel_energy_arr(Q, k, opts["prefix_bits"], workers[0])
+            if "time_arr" in use_metrics:
+                from .metrics import even_time_arr
+                share = even_time_arr(1.0, k + opts["prefix_bits"])[: 1 << opts["prefix_bits"]] * (1 << k)
+                metrics["time_arr"] = np.concatenate([ms * share for ms in task_ms])
         sol.metrics = [metrics]
-        sol.time_to_solve_ms = max(r["time_ms"] for r in results)
-        sol.worker_logs = []
-        n_tasks = self._splits_cnt
-        for w, r in enumerate(results):
-            first = w * n_tasks // len(results)
-            last = (w + 1) * n_tasks // len(results) - 1
-            sol.worker_logs.append(dict(worker_id=w, device=f"cuda:{devs[w]}", task_ids=(first, last),
-                                        time_to_solve_ms=r["time_ms"], states=r["states"]))
-        sol.search = {k2: best[k2] for k2 in ("form", "candidate_records", "pass1_ms", "pass2_ms", "order_key")}
-        sol.search["states"] = sum(r["states"] for r in results)
+        sol.time_to_solve_ms = time_to_solve
+        sol.worker_logs = logs
+        sol.search = {k2: best[k2] for k2 in ("form", "pass1_ms", "pass2_ms", "order_key")}
+        sol.search["candidate_records"] = sum(r["candidate_records"] for r in parts)
+        sol.search["states"] = sum(r["states"] for r in parts)
+        sol.search["workers"] = len(workers)
         return sol
 
     def _solve_qbf1_int16(self, problem, Q, k, json_str, t0, kwargs) -> Solution:
@@ -419,58 +490,49 @@ class Parallel(SolverABC):
         return sol
 
     @staticmethod
-    def _run_workers(devs, Q, opts, timeout, worker=None):
-        """One spawned process per device (worker, default _worker_main) searches a contiguous
-        share; the parent exchanges the pass-1 minima and collects the shares' results.  A
-        worker that reports an exception or exits without reporting raises RuntimeError; no
-        answer within ``timeout`` seconds (default 24 h, as the reference's scheduler) raises
-        TimeoutError.  Unlike the reference's scheduler (scheduler.py:26-45), partial results
-        are never merged."""
+    def _run_workers(workers, Q, opts, n_tasks, timeout, worker=None):
+        """The reference's devices_scheduler (src/qubo_lib/solvers/scheduler.py:5-45): one
+        spawned process per entry of ``workers`` (device ids, repeats allowed) takes task ids
+        0 .. n_tasks-1 from a shared queue (``worker``, default _task_worker).  Returns
+        {task: (worker_id, result)}.  A worker that reports an exception, or exits with a
+        non-zero code, raises RuntimeError; tasks still missing at ``timeout`` seconds
+        (default 24 h, as the reference's scheduler) raise TimeoutError.  Unlike the
+        reference's scheduler, partial results are never merged."""
         ctx = mp.get_context("spawn")
-        outbox = ctx.Queue()
-        inboxes = [ctx.Queue() for _ in devs]
-        target = worker or _worker_main
-        procs = [ctx.Process(target=target, args=(d, Q, opts, i, len(devs), inboxes[i], outbox))
-                 for i, d in enumerate(devs)]
+        tasks = ctx.Queue()
+        results = ctx.Queue()
+        for t in range(n_tasks):
+            tasks.put(t)
+        for _ in workers:
+            tasks.put(None)
+        target = worker or _task_worker
+        procs = [ctx.Process(target=target, args=(w, d, Q, opts, tasks, results)) for w, d in enumerate(workers)]
         for p in procs:
             p.start()
         deadline = time.time() + (timeout if timeout is not None else 24 * 3600)
-
-        def receive(done: dict):
-            while True:
+        done = {}
+        try:
+            while len(done) < n_tasks:
                 left = deadline - time.time()
                 if left <= 0:
-                    raise _queue.Empty
+                    raise TimeoutError(f"Parallel: {n_tasks - len(done)} of {n_tasks} tasks unfinished at "
+                                       f"timeout={timeout}")
                 try:
-                    kind, idx, val = outbox.get(timeout=min(0.5, left))
-                    return kind, idx, val
+                    kind, task, wid, val = results.get(timeout=min(0.5, left))
                 except _queue.Empty:
                     for i, p in enumerate(procs):
-                        if i not in done and not p.is_alive() and outbox.empty():
-                            raise RuntimeError(f"worker {i} exited (code {p.exitcode}) without a result")
-
-        try:
-            mins = {}
-            while len(mins) < len(devs):
-                kind, idx, val = receive(mins)
+                        if not p.is_alive() and p.exitcode not in (0, None) and results.empty():
+                            raise RuntimeError(f"worker {i} exited (code {p.exitcode}) without a result") from None
+                    if all(not p.is_alive() for p in procs) and results.empty():
+                        raise RuntimeError(f"workers exited with {n_tasks - len(done)} tasks unfinished") from None
+                    continue
                 if kind == "err":
-                    raise RuntimeError(f"worker {idx}: {val}")
-                mins[idx] = val
-            gmin = min(mins.values())
-            for q in inboxes:
-                q.put(gmin)
-            results = {}
-            while len(results) < len(devs):
-                kind, idx, val = receive(results)
-                if kind == "err":
-                    raise RuntimeError(f"worker {idx}: {val}")
-                results[idx] = val
-        except _queue.Empty:
-            raise TimeoutError(f"Parallel: workers did not finish within timeout={timeout}") from None
+                    raise RuntimeError(f"worker {wid} (task {task}): {val}")
+                done[task] = (wid, val)
         finally:
             for p in procs:
                 p.join(timeout=5)
                 if p.is_alive():
                     p.terminate()
                     p.join()
-        return [results[i] for i in range(len(devs))]
+        return done

@@ -1,12 +1,14 @@
 """Generate the golden fixtures in tests/golden/ by running the reference itself.
 
-Run in a container that holds the reference source (cloud-ru-tech/evo-quantum-qubolib)
-under /root/reference:
+Run in a container that holds the reference source (cloud-ru-tech/evo-quantum-qubolib),
+with QUBO_REFERENCE_ROOT naming its checkout (the directory holding src/ and
+showcase.ipynb):
 
-    python tests/golden/make_golden.py            # all fixtures (a few minutes)
-    python tests/golden/make_golden.py metrics    # metrics.json only
+    QUBO_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py           # all fixtures
+    QUBO_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py metrics   # metrics.json
+    QUBO_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py schema    # solution_schema.json
 
-The reference is imported from /root/reference/src with the test-only stubs in
+The reference is imported from <checkout>/src with the test-only stubs in
 tests/golden/refstub (jsonpickle and ortools are not installed; neither is on the search
 arithmetic).  Each fixture records the inputs (Q as integers or float bit-exact decimal
 strings), the kwargs, and what the reference returned.  Nothing here is needed at test
@@ -21,7 +23,10 @@ import sys
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC = "/root/reference/src"
+REF_ROOT = os.environ.get("QUBO_REFERENCE_ROOT", "")
+if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "src", "qubo_lib")):
+    sys.exit("set QUBO_REFERENCE_ROOT to the reference checkout (the directory holding src/qubo_lib)")
+REF_SRC = os.path.join(REF_ROOT, "src")
 STUB = os.path.join(HERE, "refstub")
 
 if os.environ.get("_QB_GOLDEN_CHILD") != "1":
@@ -180,9 +185,45 @@ def metrics_fixture():
     print("metrics", len(recs))
 
 
+def _field_types(obj) -> dict:
+    return {k: type(v).__name__ for k, v in sorted(vars(obj).items())}
+
+
+def schema_fixture():
+    """The attribute set (and value types) of the Solution objects the reference returns,
+    which is what Solution.to_json serialises (jsonpickle writes an object's __dict__ under a
+    py/object tag, src/qubo_lib/solution.py:64-69): QBF with and without use_metrics, a
+    reduced problem (prefix_E), and Parallel(QBF) with its worker_logs."""
+    rng = np.random.default_rng(77)
+    U = rng.integers(-30, 31, (12, 12)).astype(np.int32)
+    Q = np.triu(U) + np.triu(U, 1).T
+    out = {}
+    sol = QBF().solve(Just_Q(Q), A=3)
+    out["qbf"] = {"fields": _field_types(sol), "metrics": [sorted(m) for m in sol.metrics],
+                  "timer_labels": sorted({lbl for _, lbl in sol.timer})}
+    sol = QBF().solve(Just_Q(Q), A=3, use_metrics="all")
+    out["qbf_metrics"] = {"fields": _field_types(sol),
+                          "metrics": {k: [type(v).__name__, str(v.dtype), list(v.shape)]
+                                      for k, v in sorted(sol.metrics[0].items())}}
+    sol = QBF().solve(ReducedProblem(Just_Q(Q), np.array([1, 0])), A=2)
+    out["qbf_reduced"] = {"fields": _field_types(sol)}
+    sol = Parallel(base_solver=QBF, splits_cnt=4, devices=["cpu"] * 2).solve(Just_Q(Q), A=2, use_metrics="all")
+    out["parallel"] = {"fields": _field_types(sol),
+                       "worker_log_fields": sorted(sol.worker_logs[0]),
+                       "worker_logs": len(sol.worker_logs),
+                       "metrics": {k: [type(v).__name__, str(v.dtype), list(v.shape)]
+                                   for k, v in sorted(sol.metrics[0].items())}}
+    json.dump({"source": "attribute sets of the reference's Solution objects (QBF, Parallel(QBF) on CPU)",
+               "cases": out}, open(os.path.join(HERE, "solution_schema.json"), "w"), indent=1)
+    print("schema", sorted(out))
+
+
 def main():
     if sys.argv[1:] == ["metrics"]:
         metrics_fixture()
+        return
+    if sys.argv[1:] == ["schema"]:
+        schema_fixture()
         return
     out = {}
     # ------------------------------------------------------------------ QBF small
@@ -264,7 +305,7 @@ def main():
     print("generators done")
 
     # ------------------------------------------------------------------ notebook goldens
-    nb = json.load(open("/root/reference/showcase.ipynb"))
+    nb = json.load(open(os.path.join(REF_ROOT, "showcase.ipynb")))
     nbrec = []
     for c in nb["cells"]:
         if c["cell_type"] != "code":

@@ -133,10 +133,12 @@ def test_config2_full_oracle():
 
 def test_maxcut_test_instance_known_answer():
     """MaxCut 'test' (10 vertices, best cut 19) from the reference's bundled data; loaded at
-    run time when the reference source is present, never stored in this repository."""
-    path = "/root/reference/src/qubo_lib/problems/well_known_instances/MaxCut.zip"
-    if not os.path.exists(path):
-        pytest.skip("reference data not present")
+    run time when QUBO_REFERENCE_ROOT names a reference checkout, never stored in this
+    repository."""
+    root = os.environ.get("QUBO_REFERENCE_ROOT", "")
+    path = os.path.join(root, "src", "qubo_lib", "problems", "well_known_instances", "MaxCut.zip")
+    if not root or not os.path.exists(path):
+        pytest.skip("reference data not present (set QUBO_REFERENCE_ROOT)")
     import zipfile
     with zipfile.ZipFile(path) as z:
         text = z.read("instance/test/test.txt").decode()
