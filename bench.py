@@ -298,6 +298,8 @@ def bench_ours(args):
     }
     if rank == 0 and world == 1:
         line["cpu_baseline"] = cpu_baseline(Q)
+        # the batch configuration (4096 small problems, one graph launch per batch) beside it
+        line["batch"] = batch_measure(max(10, min(args.steps, 20)), args.warmup, with_baselines=False)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -324,57 +326,93 @@ def bench_case(args):
                   flush=True)
 
 
-def bench_batch(args):
+BATCH_WORKLOAD = "4096 float32 QUBOs, n uniform in [16, 28], Q = (G + G^T)/2, G ~ N(0,1), seeds 0..4095"
+
+
+def batch_measure(steps: int, warmup: int, with_baselines: bool) -> dict:
     """The 4096-instance batch (n uniform in [16, 28], float Q = (G + G^T) / 2 with G normal,
-    seeds 0..4095): states/s of one batched search (qb_solve_batch) over all instances,
-    against a one-call-per-problem loop over a sample and the oracle's CPU restatement of
-    the reference over a sample (both scaled by their share of the states)."""
-    import numpy as np
+    seeds 0..4095), solved with qb_solve_batch as one CUDA graph launch per batch.  Device time
+    by CUDA events around the graph launch (max of nothing: one GPU); e2e = wall time of the
+    public call with host-resident matrices (packing, H2D, the graph, D2H, decoding).  The
+    roofline fraction covers the tensor-core pass-1 kernels of the launch-by-launch run (the
+    instances with n >= 24; 32 flop per state), against the measured bf16 peak and against the
+    int8 dense peak (twice the bf16 figure, the B200's nominal ratio)."""
     import torch
     import qubo_b200  # noqa: F401
     from qubo_b200 import _lib, configs
-    torch.cuda.set_device(0)
     Qs = configs.batch_f32(4096)
     states = sum(1 << q.shape[0] for q in Qs)
+    tc_states = sum(1 << q.shape[0] for q in Qs if q.shape[0] >= 24)
     h = _lib.handle(0)
     stream = torch.cuda.current_stream(0).cuda_stream
-    for _ in range(args.warmup):
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:0")
+    for _ in range(max(3, warmup)):
+        h.solve_batch(Qs, stream=stream, graph=True)
         h.solve_batch(Qs, stream=stream)
-    dev_ms, wall = [], []
-    for _ in range(args.steps):
+    g_ms, wall, p_ms, k_ms = [], [], [], []
+    res = None
+    for _ in range(steps):
+        flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = h.solve_batch(Qs, stream=stream)
+        res = h.solve_batch(Qs, stream=stream, graph=True)
         wall.append(time.perf_counter() - t0)
-        dev_ms.append(res[0]["pass1_ms"] + res[0]["pass2_ms"])
-    sample = Qs[::16]
-    s_states = sum(1 << q.shape[0] for q in sample)
-    t0 = time.perf_counter()
-    for q in sample:
-        h.solve(q, stream=stream)
-    loop_s = time.perf_counter() - t0
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    cpu = Qs[::256]
-    c_states = sum(1 << q.shape[0] for q in cpu)
-    t0 = time.perf_counter()
-    for q in cpu:
-        oracle.qbf_port(q)
-    cpu_s = time.perf_counter() - t0
-    ms = statistics.median(dev_ms)
-    line = {"metric": "states/s (4096-instance batch, exact FP64 argmin each)", "value": states / (ms * 1e-3),
-            "unit": "states/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 re-scoring)",
-            "data": "synthetic",
-            "config": {"workload": "4096 float32 QUBOs, n uniform in [16, 28], Q = (G + G^T)/2, G ~ N(0,1), seeds 0..4095",
-                       "states_per_step": states, "instances": len(Qs)},
-            "e2e": {"value": states / statistics.median(wall), "unit": "states/s",
-                    "h2d_bytes_per_step": int(res[0]["h2d_bytes"]), "d2h_bytes_per_step": int(res[0]["d2h_bytes"])},
-            "gpu_launches": int(res[0]["kernels"]),
-            "one_call_per_problem": {"value": s_states / loop_s, "unit": "states/s",
-                                     "sample": f"{len(sample)} instances (every 16th), {loop_s:.2f} s"},
-            "cpu_baseline": {"value": c_states / cpu_s, "unit": "states/s", "cores": 1, "kind": "port",
-                             "sample": f"{len(cpu)} instances (every 256th), QBF B = 20 prefix loop, {cpu_s:.1f} s"}}
+        g_ms.append(res[0]["pass1_ms"])
+    for _ in range(steps):
+        flush.zero_()
+        r2 = h.solve_batch(Qs, stream=stream)
+        p_ms.append(r2[0]["pass1_ms"] + r2[0]["pass2_ms"])
+        k_ms.append(r2[0]["kernel_ms"])
+    ms = statistics.median(g_ms)
+    peak, _, peak_kind = _peaks()
+    kms = statistics.median(k_ms)
+    tflops = tc_states * FLOPS_PER_STATE_TC / (kms * 1e-3) / 1e12
+    out = {"metric": "states/s (4096-instance batch, exact FP64 argmin each)", "value": states / (ms * 1e-3),
+           "unit": "states/s", "steps": steps, "warmup": max(3, warmup), "ms_per_step": ms,
+           "dtype": "f32 (f16 digit operands, fp32 accumulate; FP64 re-scoring)",
+           "config": {"workload": BATCH_WORKLOAD, "states_per_step": states, "instances": len(Qs),
+                      "launch": "one CUDA graph (uploads, six kernels, result copy)",
+                      "l2": "flushed between steps (256 MiB write)"},
+           "e2e": {"value": states / statistics.median(wall), "unit": "states/s",
+                   "h2d_bytes_per_step": int(res[0]["h2d_bytes"]), "d2h_bytes_per_step": int(res[0]["d2h_bytes"])},
+           "gpu_launches": int(res[0]["kernels"]),
+           "launch_by_launch": {"ms_per_step": statistics.median(p_ms), "value": states / (statistics.median(p_ms) * 1e-3)},
+           "roofline": {"bound": "tensor", "kernel": "pass-1 kernels (tensor-core items n >= 24, Gray items below)",
+                        "kernel_ms": kms, "achieved": tflops, "unit": "TFLOP/s", "tc_states": tc_states,
+                        "flops_per_state": FLOPS_PER_STATE_TC,
+                        "frac_bf16": tflops / peak, "peak_bf16": peak, "peak_bf16_kind": f"bf16 dense burst, {peak_kind}",
+                        "frac_int8": tflops / (2 * peak), "peak_int8": 2 * peak,
+                        "peak_int8_kind": "2 x the bf16 figure (nominal dense int8 : bf16 ratio)"}}
+    if with_baselines:
+        sample = Qs[::16]
+        s_states = sum(1 << q.shape[0] for q in sample)
+        t0 = time.perf_counter()
+        for q in sample:
+            h.solve(q, stream=stream)
+        loop_s = time.perf_counter() - t0
+        out["one_call_per_problem"] = {"value": s_states / loop_s, "unit": "states/s",
+                                       "sample": f"{len(sample)} instances (every 16th), {loop_s:.2f} s"}
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        cpu = Qs[::256]
+        c_states = sum(1 << q.shape[0] for q in cpu)
+        t0 = time.perf_counter()
+        for q in cpu:
+            oracle.qbf_port(q)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": c_states / cpu_s, "unit": "states/s", "cores": 1, "kind": "port",
+                               "sample": f"{len(cpu)} instances (every 256th), QBF B = 20 prefix loop, {cpu_s:.1f} s"}
+    return out
+
+
+def bench_batch(args):
+    """The 4096-instance batch as its own line (python bench.py --case batch)."""
+    import torch
+    torch.cuda.set_device(0)
+    b = batch_measure(args.steps, args.warmup, with_baselines=True)
+    line = dict(b)
+    line.update({"n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "data": "synthetic"})
     print(json.dumps(line), flush=True)
 
 

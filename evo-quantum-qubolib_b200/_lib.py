@@ -21,6 +21,7 @@ FORM_NAMES = {v: k for k, v in FORMS.items()}
 FORM_NAMES[4] = "qb_f1_int16"
 QB_FLAG_INT16_WRAP = 1
 QB_FLAG_TEST_STALL = 2
+QB_FLAG_GRAPH = 4
 TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
 
 _DTYPES = {
@@ -50,7 +51,9 @@ class QbResult(ctypes.Structure):
                 ("states", ctypes.c_int64), ("candidate_records", ctypes.c_int64), ("form_used", ctypes.c_int32),
                 ("is_integer", ctypes.c_int32), ("found", ctypes.c_int32), ("status", ctypes.c_int32),
                 ("pass1_ms", ctypes.c_float), ("pass2_ms", ctypes.c_float), ("kernels", ctypes.c_int32),
-                ("kernel_ms", ctypes.c_float), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+                ("kernel_ms", ctypes.c_float), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+                ("rec_log2", ctypes.c_int32), ("suffix_bits", ctypes.c_int32), ("unit_log2", ctypes.c_int32),
+                ("tuned", ctypes.c_int32)]
 
 
 class QbNoAllocResult(ctypes.Structure):
@@ -148,11 +151,11 @@ class Handle:
 
     @staticmethod
     def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
-                max_candidates=0, stream=None, int16_wrap=False, flags=0) -> QbOptions:
+                max_candidates=0, stream=None, int16_wrap=False, flags=0, graph=False) -> QbOptions:
         return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
                          prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
                          max_candidates=int(max_candidates),
-                         flags=int(flags) | (QB_FLAG_INT16_WRAP if int16_wrap else 0),
+                         flags=int(flags) | (QB_FLAG_INT16_WRAP if int16_wrap else 0) | (QB_FLAG_GRAPH if graph else 0),
                          stream=stream)
 
     def solve(self, Q: np.ndarray, **opts) -> dict:
@@ -201,50 +204,37 @@ class Handle:
             _raise(rc, "qb_solve_finish")
         return result_dict(r, n)
 
-    def solve_batch(self, Qs: list, **opts) -> list[dict]:
+    def solve_batch(self, Qs: list, **opts) -> "BatchResults":
+        """qb_solve_batch over the matrices Qs; returns a BatchResults (a sequence of per-problem
+        result dicts, decoded on access, with every field also available as one array)."""
         count = len(Qs)
         probs = (QbProblem * count)()
-        keep = [np.ascontiguousarray(Q) for Q in Qs]
+        keep = [Q if (isinstance(Q, np.ndarray) and Q.flags.c_contiguous) else np.ascontiguousarray(Q) for Q in Qs]
+        meta = []
         for Q in keep:
-            if Q.ndim != 2 or Q.shape[0] != Q.shape[1]:
-                raise ValueError(f"Q must be square, got shape {Q.shape}")
-            if Q.dtype not in _DTYPES:
+            sh = Q.shape
+            if len(sh) != 2 or sh[0] != sh[1]:
+                raise ValueError(f"Q must be square, got shape {sh}")
+            code = _DTYPES.get(Q.dtype)
+            if code is None:
                 raise TypeError(f"unsupported Q dtype {Q.dtype}")
-        # the problem descriptors filled column by column through a structured view
-        ns = np.fromiter((q.shape[0] for q in keep), dtype=np.int64, count=count)
+            meta.append((sh[0], code, Q.__array_interface__["data"][0]))
+        ns = np.fromiter((m[0] for m in meta), dtype=np.int64, count=count)
         if count:
+            # the problem descriptors filled column by column through a structured view
             view = np.frombuffer(probs, dtype=np.dtype(QbProblem))
             view["n"] = ns
             view["ldq"] = ns
-            view["dtype"] = np.fromiter((_DTYPES[q.dtype] for q in keep), dtype=np.int32, count=count)
-            view["q"] = np.fromiter((q.__array_interface__["data"][0] for q in keep), dtype=np.uint64, count=count)
+            view["dtype"] = np.fromiter((m[1] for m in meta), dtype=np.int32, count=count)
+            view["q"] = np.fromiter((m[2] for m in meta), dtype=np.uint64, count=count)
         o = self.options(**opts)
         res = (QbResult * count)()
         rc = load().qb_solve_batch(self._h, probs, count, ctypes.byref(o), res)
         if rc:
             _raise(rc, "qb_solve_batch")
         if not count:
-            return []
-        # decoded together: one structured array, the state bits grouped by size
-        arr = np.frombuffer(res, dtype=np.dtype(QbResult))
-        xs = arr["best_x"].astype(np.uint64)
-        bits = [None] * count
-        for n in np.unique(ns):
-            idx = np.flatnonzero(ns == n)
-            sh = np.arange(int(n) - 1, -1, -1, dtype=np.uint64)
-            mat = ((xs[idx][:, None] >> sh[None, :]) & np.uint64(1)).astype(np.int32)
-            for row, i in enumerate(idx):
-                bits[i] = mat[row]
-        c = {name: arr[name].tolist() for name, _ in QbResult._fields_}
-        forms = [FORM_NAMES.get(f, str(f)) for f in c["form_used"]]
-        return [{
-            "found": bool(c["found"][i]), "best_X_int": c["best_x"][i], "best_X": bits[i],
-            "best_E": c["best_e"][i], "best_E_int": c["best_e_int"][i], "order_key": c["order_key"][i],
-            "pass1_min": c["pass1_min"][i], "err_bound": c["err_bound"][i], "states": c["states"][i],
-            "candidate_records": c["candidate_records"][i], "form": forms[i], "is_integer": bool(c["is_integer"][i]),
-            "pass1_ms": c["pass1_ms"][i], "pass2_ms": c["pass2_ms"][i], "kernels": c["kernels"][i],
-            "kernel_ms": c["kernel_ms"][i], "h2d_bytes": c["h2d_bytes"][i], "d2h_bytes": c["d2h_bytes"][i],
-        } for i in range(count)]
+            return BatchResults(np.zeros(0, dtype=np.dtype(QbResult)), ns)
+        return BatchResults(np.frombuffer(res, dtype=np.dtype(QbResult)).copy(), ns)
 
     def prefix_minima(self, Q: np.ndarray, prefix_bits: int = -1) -> np.ndarray:
         """Per-prefix minimum energies in QBF's Gray visiting order (qb_prefix_minima)."""
@@ -268,6 +258,78 @@ class Handle:
         return FORM_NAMES[f.value]
 
 
+class BatchResults:
+    """Results of qb_solve_batch: ``results[i]`` is problem i's result dict (the keys of
+    result_dict), built when it is first read; ``results.field(name)`` is one field of every
+    problem as an array, and ``results.best_X_int`` / ``results.best_E`` are shortcuts."""
+
+    def __init__(self, arr: np.ndarray, ns: np.ndarray):
+        self._arr = arr
+        self._ns = ns
+        self._cache = {}
+
+    def __len__(self) -> int:
+        return len(self._arr)
+
+    def __iter__(self):
+        return (self[i] for i in range(len(self)))
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[j] for j in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        d = self._cache.get(i)
+        if d is None:
+            r = self._arr[i]
+            d = result_row(r, int(self._ns[i]))
+            self._cache[i] = d
+        return d
+
+    def __eq__(self, other):
+        if isinstance(other, (list, tuple)):
+            return list(self) == list(other)
+        return NotImplemented
+
+    def field(self, name: str) -> np.ndarray:
+        return self._arr[name]
+
+    @property
+    def best_X_int(self) -> np.ndarray:
+        return self._arr["best_x"]
+
+    @property
+    def best_E(self) -> np.ndarray:
+        return self._arr["best_e"]
+
+
+def result_row(r, n: int) -> dict:
+    """result_dict of one row of a structured QbResult array."""
+    x = int(r["best_x"])
+    return {
+        "found": bool(r["found"]),
+        "best_X_int": x,
+        "best_X": np.array([(x >> (n - 1 - i)) & 1 for i in range(n)], dtype=np.int32),
+        "best_E": float(r["best_e"]),
+        "best_E_int": int(r["best_e_int"]),
+        "order_key": int(r["order_key"]),
+        "pass1_min": float(r["pass1_min"]),
+        "err_bound": float(r["err_bound"]),
+        "states": int(r["states"]),
+        "candidate_records": int(r["candidate_records"]),
+        "form": FORM_NAMES.get(int(r["form_used"]), str(int(r["form_used"]))),
+        "is_integer": bool(r["is_integer"]),
+        "pass1_ms": float(r["pass1_ms"]),
+        "pass2_ms": float(r["pass2_ms"]),
+        "kernels": int(r["kernels"]),
+        "kernel_ms": float(r["kernel_ms"]),
+        "h2d_bytes": int(r["h2d_bytes"]),
+        "d2h_bytes": int(r["d2h_bytes"]),
+        "plan": {"rec_log2": int(r["rec_log2"]), "suffix_bits": int(r["suffix_bits"]),
+                 "unit_log2": int(r["unit_log2"]), "tuned": bool(r["tuned"])},
+    }
+
+
 def result_dict(r: QbResult, n: int) -> dict:
     x = int(r.best_x)
     return {
@@ -289,6 +351,8 @@ def result_dict(r: QbResult, n: int) -> dict:
         "kernel_ms": float(r.kernel_ms),
         "h2d_bytes": int(r.h2d_bytes),
         "d2h_bytes": int(r.d2h_bytes),
+        "plan": {"rec_log2": int(r.rec_log2), "suffix_bits": int(r.suffix_bits), "unit_log2": int(r.unit_log2),
+                 "tuned": bool(r.tuned)},
     }
 
 

@@ -73,6 +73,26 @@ constexpr double kTwo53 = 9007199254740992.0;
 constexpr int kPrefixMinimaMaxA = 26;  // qb_prefix_minima: at most 2^26 prefixes (512 MiB of results)
 constexpr int kDefaultCap = 1 << 16;
 
+// Gray-form split: suffix bits b (>= 13), prefix a = n - b, 2^sbits prefix steps per record,
+// 2^ubits prefix steps per work unit
+struct GrayShape {
+  int a, b, cbbits, sbits, ubits;
+};
+
+// the default shape for n, or the one with suffix bits b / record steps 2^sbits when those are
+// given (0 = default) and valid: 13 <= b, 7 <= a <= 24, 5 <= sbits <= a
+inline GrayShape gray_shape(int n, int b_want = 0, int sbits_want = 0) {
+  GrayShape g;
+  g.b = std::max(13, n - 16);
+  if (b_want >= 13 && n - b_want >= 7 && n - b_want <= 24) g.b = b_want;
+  g.a = n - g.b;
+  g.cbbits = g.b - 13;
+  g.sbits = std::min(g.a, std::max(5, n - 34));
+  if (sbits_want >= 5 && sbits_want <= g.a) g.sbits = sbits_want;
+  g.ubits = std::min(g.a, std::max(7, std::max(g.sbits, std::min(g.a, g.a + g.cbbits - 11))));
+  return g;
+}
+
 struct Plan {
   int n = 0;
   bool is_int = false;
@@ -101,6 +121,12 @@ struct qb_handle_s {
   DevBuf bat[14];  // qb_solve_batch: W, insts, gtab items, unit items, selection ids, cands, out, G tables,
                    // records, minima, scaled W, tensor-core items, item ranges, error word
   HostBuf hW, hmisc, hout, hbat;  // hbat: qb_solve_batch's packed W matrices (pinned)
+  HostBuf hstage;                  // qb_solve_batch: descriptors and work lists (pinned)
+  // qb_solve_batch with QB_FLAG_GRAPH: the captured launch sequence of the last batch and
+  // the fingerprint (shapes, options, buffer addresses) it is valid for
+  cudaGraphExec_t batch_graph = nullptr;
+  std::vector<uint64_t> batch_graph_key;
+  int batch_graph_kernels = 0;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // 4, 5: main kernel
   int64_t h2d = 0, d2h = 0;  // bytes copied by the current call
   float kernel_ms = 0.f;
@@ -113,7 +139,13 @@ struct qb_handle_s {
   double local_min = 0.0;
   int64_t exact_count = 0;  // EXACT form: records evaluated in pass 1
   int cap = kDefaultCap;
-  int autotuned_form[qb::kMaxN + 1] = {0};
+  // qb_autotune's choices per (dtype class: 0 float, 1 integer; n); 0 fields = defaults
+  struct Tuned {
+    int form = 0;
+    int tc_gl = 0;
+    int gray_b = 0, gray_sbits = 0;
+  };
+  Tuned tuned[2][qb::kMaxN + 1];
 };
 
 namespace {
@@ -249,7 +281,7 @@ int choose_form(qb_handle* h, const Plan& P, int requested) {
   if (requested == QB_FORM_TC) return tc_ok ? QB_FORM_TC : -1;
   if (requested == QB_FORM_GRAY) return P.n >= 20 ? QB_FORM_GRAY : -1;
   // auto
-  if (h->autotuned_form[P.n]) return h->autotuned_form[P.n];
+  if (h->tuned[P.is_int ? 1 : 0][P.n].form) return h->tuned[P.is_int ? 1 : 0][P.n].form;
   if (tc_ok) return QB_FORM_TC;
   if (P.n >= 20) return QB_FORM_GRAY;
   return QB_FORM_EXACT;
@@ -277,13 +309,10 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
     P.eps = 0.0;
     return QB_OK;
   }
+  const qb_handle::Tuned& T = h->tuned[P.is_int ? 1 : 0][n];
   if (form == QB_FORM_GRAY) {
-    int b = std::max(13, n - 16);
-    int a = n - b;
-    int cbbits = b - 13;
-    int sbits = std::min(a, std::max(5, n - 34));
-    int ubits = std::max(7, std::max(sbits, std::min(a, a + cbbits - 11)));
-    ubits = std::min(ubits, a);
+    const GrayShape gs = gray_shape(n, T.gray_b, T.gray_sbits);
+    const int a = gs.a, b = gs.b, cbbits = gs.cbbits, sbits = gs.sbits, ubits = gs.ubits;
     P.a = a;
     P.b = b;
     P.ubits = ubits;
@@ -302,7 +331,7 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
     return QB_OK;
   }
   // tensor-core form
-  qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc);
+  qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc, T.tc_gl);
   P.tc.stall = (o->flags & QB_FLAG_TEST_STALL) != 0;
   P.geom.kind = qb::kGeomTC;
   P.geom.gl = P.tc.gl;
@@ -311,6 +340,28 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
   P.states = P.tc.states;
   P.eps = P.tc.eps;
   return QB_OK;
+}
+
+// the plan parameters a result reports
+void fill_plan_fields(const qb_handle* h, const Plan& P, qb_result* r) {
+  const qb_handle::Tuned& T = h->tuned[P.is_int ? 1 : 0][P.n];
+  if (P.form == QB_FORM_GRAY) {
+    r->rec_log2 = P.geom.sbits;
+    r->suffix_bits = P.b;
+    r->unit_log2 = P.ubits;
+    r->tuned = (T.gray_b || T.gray_sbits) ? 1 : 0;
+  } else if (P.form == QB_FORM_TC) {
+    r->rec_log2 = P.tc.gl;
+    r->suffix_bits = 15;
+    r->unit_log2 = 0;
+    r->tuned = T.tc_gl ? 1 : 0;
+  } else {
+    r->rec_log2 = P.geom.fbits;
+    r->suffix_bits = 0;
+    r->unit_log2 = 0;
+    r->tuned = 0;
+  }
+  if (T.form && T.form == P.form) r->tuned = 1;
 }
 
 int upload_W(qb_handle* h, const std::vector<double>& W) {
@@ -444,6 +495,8 @@ int qb_handle_destroy(qb_handle* h) {
   h->hmisc.release();
   h->hout.release();
   h->hbat.release();
+  h->hstage.release();
+  if (h->batch_graph) cudaGraphExecDestroy(h->batch_graph);
   for (auto& ev : h->ev)
     if (ev) cudaEventDestroy(ev);
   if (h->own) cudaStreamDestroy(h->own);
@@ -607,6 +660,7 @@ int solve_fused(qb_handle* h, const Plan& P, qb_result* r) {
   r->kernels = h->kernels;
   r->h2d_bytes = h->h2d;
   r->d2h_bytes = h->d2h;
+  fill_plan_fields(h, P, r);
   r->status = QB_OK;
   return QB_OK;
 }
@@ -772,6 +826,7 @@ int qb_solve_finish(qb_handle* h, double global_min, qb_result* r) {
   r->kernel_ms = h->kernel_ms;
   r->h2d_bytes = h->h2d;
   r->d2h_bytes = h->d2h;
+  fill_plan_fields(h, P, r);
   r->status = QB_OK;
   return QB_OK;
 }
@@ -941,14 +996,27 @@ constexpr int kBatchMaxN = 36;            // larger problems are solved one by o
 constexpr int kBatchTcMinN = 24;          // from here on the tensor-core form (>= 512 tiles)
 constexpr uint64_t kBatchGtabChunk = 1024;  // G-table steps per CTA
 
-template <class T>
-int upload_vec(qb_handle* h, DevBuf& d, const std::vector<T>& v) {
-  const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
-  QB_CUDA(d.ensure(bytes));
-  if (!v.empty()) {
-    QB_CUDA(cudaMemcpyAsync(d.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->st));
-    h->h2d += (int64_t)(v.size() * sizeof(T));
+// Host -> device copies of qb_solve_batch's small arrays, staged in one pinned buffer so that
+// every copy reads from a stable address (a captured graph replays the same copies)
+struct Stage {
+  struct Copy {
+    void* dst;
+    size_t off, bytes;
+  };
+  std::vector<unsigned char> bytes;  // assembled here, then copied into the pinned buffer once
+  std::vector<Copy> copies;
+  template <class T>
+  void add(void* dst, const std::vector<T>& v) {
+    const size_t off = (bytes.size() + 15) & ~(size_t)15;
+    bytes.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+    if (!v.empty()) copies.push_back(Copy{dst, off, v.size() * sizeof(T)});
   }
+};
+
+template <class T>
+int ensure_for(DevBuf& d, const std::vector<T>& v) {
+  QB_CUDA(d.ensure(std::max<size_t>(v.size() * sizeof(T), 16)));
   return QB_OK;
 }
 
@@ -1012,9 +1080,13 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     I.w_off = w_used;
     w_used += (uint64_t)n * n;
     int free_bits;
-    if (n >= kBatchTcMinN && tc_allowed && qb::tc_supported(n)) {
+    const qb_handle::Tuned& T = h->tuned[is_int ? 1 : 0][n];
+    // the tuned form of (dtype class, n) when qb_autotune chose one, else tensor-core from 24
+    const bool use_tc = tc_allowed && qb::tc_supported(n) &&
+                        (T.form ? T.form == QB_FORM_TC : n >= kBatchTcMinN);
+    if (use_tc) {
       qb::TcPlan tp;
-      qb::tc_plan(n, is_int, abs_sum, 0, 1, &tp);
+      qb::tc_plan(n, is_int, abs_sum, 0, 1, &tp, T.tc_gl);
       I.kind = qb::kBatchTC;
       I.gl = tp.gl;
       I.exact_digits = tp.exact ? 1 : 0;
@@ -1032,11 +1104,12 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     } else if (n >= 20) {
       any_gray = true;
       I.kind = qb::kBatchGray;
-      I.b = std::max(13, n - 16);
-      I.a = n - I.b;
-      I.cbbits = I.b - 13;
-      I.sbits = std::min(I.a, std::max(5, n - 34));
-      const int ubits = std::min(I.a, std::max(7, std::max(I.sbits, std::min(I.a, I.a + I.cbbits - 11))));
+      const GrayShape gs = gray_shape(n, T.gray_b, T.gray_sbits);
+      I.b = gs.b;
+      I.a = gs.a;
+      I.cbbits = gs.cbbits;
+      I.sbits = gs.sbits;
+      const int ubits = gs.ubits;
       I.gubits = ubits - I.sbits;
       const uint64_t units = 1ull << (I.a - ubits + I.cbbits);
       I.nrec = units << (I.gubits + 3);
@@ -1063,60 +1136,18 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   // candidate list: the small problems' records first, then room for the Gray problems'
   const int prefilled = (int)pre.size();
   const int cap = prefilled + std::max(4096, 8 * (int)gray_ids.size());
-  // device buffers
   DevBuf* B = h->bat;
   int rc;
-  QB_CUDA(B[0].ensure(std::max<uint64_t>(w_used, 2) * sizeof(double)));
-  QB_CUDA(cudaMemcpyAsync(B[0].p, Wall, w_used * sizeof(double), cudaMemcpyHostToDevice, h->st));
-  h->h2d += (int64_t)(w_used * sizeof(double));
-  if ((rc = upload_vec(h, B[1], insts))) return rc;
-  if ((rc = upload_vec(h, B[2], gitems))) return rc;
-  if ((rc = upload_vec(h, B[3], uitems))) return rc;
-  if ((rc = upload_vec(h, B[4], gray_ids))) return rc;
-  QB_CUDA(B[5].ensure((size_t)cap * sizeof(qb::BatchCand)));  // room first: ensure() may reallocate
-  if ((rc = upload_vec(h, B[5], pre))) return rc;
-  QB_CUDA(B[6].ensure((size_t)cap * sizeof(qb::ExactOut)));
-  QB_CUDA(B[7].ensure(std::max<uint64_t>(gtab_total, 4) * sizeof(float)));
-  QB_CUDA(B[8].ensure(std::max<uint64_t>(rec_total, 4) * sizeof(float)));
-  // minima: emin[m], kmin[m] (uint64), pass1_min[m] (float), cand_count (int)
-  const size_t mb = (size_t)m * 8;
-  QB_CUDA(B[9].ensure(2 * mb + (size_t)m * 4 + 16));
-  uint64_t* emin = static_cast<uint64_t*>(B[9].p);
-  uint64_t* kmin = emin + m;
-  float* p1min = reinterpret_cast<float*>(kmin + m);
-  int* ccount = reinterpret_cast<int*>(static_cast<char*>(B[9].p) + 2 * mb + (size_t)m * 4);
-  QB_CUDA(cudaMemsetAsync(B[9].p, 0xff, 2 * mb, h->st));
-  QB_CUDA(h->hmisc.ensure(64));
-  *static_cast<int*>(h->hmisc.p) = prefilled;
-  QB_CUDA(cudaMemcpyAsync(ccount, h->hmisc.p, sizeof(int), cudaMemcpyHostToDevice, h->st));
-  h->h2d += (int64_t)sizeof(int);
-  const double* dW = static_cast<const double*>(B[0].p);
-  const qb::BatchInst* dI = static_cast<const qb::BatchInst*>(B[1].p);
-  qb::BatchCand* dC = static_cast<qb::BatchCand*>(B[5].p);
-  qb::ExactOut* dO = static_cast<qb::ExactOut*>(B[6].p);
-  QB_CUDA(cudaEventRecord(h->ev[0], h->st));
-  QB_CUDA(cudaEventRecord(h->ev[4], h->st));
-  if (any_gray) {
-    QB_CUDA(cudaFuncSetAttribute(qb::batch_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gtab));
-    qb::batch_gtab_kernel<<<(unsigned)gitems.size(), 256, sm_gtab, h->st>>>(
-        dI, static_cast<const qb::BatchItem*>(B[2].p), dW, static_cast<float*>(B[7].p));
-    QB_CUDA(cudaFuncSetAttribute(qb::batch_gray_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gray));
-    qb::batch_gray_kernel<<<(unsigned)uitems.size(), qb::kGrayThreads, sm_gray, h->st>>>(
-        dI, static_cast<const qb::BatchItem*>(B[3].p), dW, static_cast<const float*>(B[7].p),
-        static_cast<float*>(B[8].p));
-    h->kernels += 2;
-  }
-  unsigned* tc_err = nullptr;
+  // the tensor-core problems' record blocks, dealt out as contiguous runs to one persistent
+  // CTA per SM (a run may span problems: one item per problem piece)
+  std::vector<qb::TcItem> items;
+  std::vector<std::pair<uint64_t, uint64_t>> offs;  // (scaled-W offset, record offset) per item
+  std::vector<uint32_t> first(1, 0);
   if (!tcs.empty()) {
-    // the tensor-core problems' record blocks, dealt out as contiguous runs to one persistent
-    // CTA per SM (a run may span problems: one item per problem piece)
     uint64_t total = 0;
     for (auto& t : tcs) total += 1ull << (insts[t.first].n - 15 - insts[t.first].gl);
     const uint64_t ctas = std::min<uint64_t>((uint64_t)h->sm_count, total);
     const uint64_t per = (total + ctas - 1) / ctas;
-    std::vector<qb::TcItem> items;
-    std::vector<std::pair<uint64_t, uint64_t>> offs;  // (scaled-W offset, record offset) per item
-    std::vector<uint32_t> first(1, 0);
     uint64_t left = per;
     for (auto& t : tcs) {
       const qb::BatchInst& I = insts[t.first];
@@ -1142,49 +1173,173 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
       }
     }
     if (first.back() != (uint32_t)items.size()) first.push_back((uint32_t)items.size());
-    // device addresses
+  }
+  // every device and pinned host allocation happens here, before any copy or launch is issued
+  QB_CUDA(B[0].ensure(std::max<uint64_t>(w_used, 2) * sizeof(double)));
+  if ((rc = ensure_for(B[1], insts))) return rc;
+  if ((rc = ensure_for(B[2], gitems))) return rc;
+  if ((rc = ensure_for(B[3], uitems))) return rc;
+  if ((rc = ensure_for(B[4], gray_ids))) return rc;
+  QB_CUDA(B[5].ensure((size_t)cap * sizeof(qb::BatchCand)));
+  QB_CUDA(B[6].ensure((size_t)cap * sizeof(qb::ExactOut)));
+  QB_CUDA(B[7].ensure(std::max<uint64_t>(gtab_total, 4) * sizeof(float)));
+  QB_CUDA(B[8].ensure(std::max<uint64_t>(rec_total, 4) * sizeof(float)));
+  // minima: emin[m], kmin[m] (uint64), pass1_min[m] (float), cand_count (int)
+  const size_t mb = (size_t)m * 8;
+  const size_t res_bytes = 2 * mb + (size_t)m * 4 + sizeof(int);
+  QB_CUDA(B[9].ensure(res_bytes + 16));
+  if (!tcs.empty()) {
     QB_CUDA(B[10].ensure(std::max<uint64_t>(wtc_used, 2) * sizeof(double)));
-    for (size_t k = 0; k < items.size(); ++k) {
-      items[k].W = static_cast<const double*>(B[10].p) + offs[k].first;
-      items[k].rec = static_cast<float*>(B[8].p) + offs[k].second;
-    }
-    QB_CUDA(cudaMemcpyAsync(B[10].p, Wtc, wtc_used * sizeof(double), cudaMemcpyHostToDevice, h->st));
-    h->h2d += (int64_t)(wtc_used * sizeof(double));
-    if ((rc = upload_vec(h, B[11], items))) return rc;
-    if ((rc = upload_vec(h, B[12], first))) return rc;
+    if ((rc = ensure_for(B[11], items))) return rc;
+    if ((rc = ensure_for(B[12], first))) return rc;
     QB_CUDA(B[13].ensure(16));
-    tc_err = static_cast<unsigned*>(B[13].p);
-    QB_CUDA(cudaMemsetAsync(tc_err, 0, 16, h->st));
-    qb::TcParams P{};
+  }
+  QB_CUDA(h->hout.ensure(res_bytes + 16));
+  uint64_t* emin = static_cast<uint64_t*>(B[9].p);
+  uint64_t* kmin = emin + m;
+  float* p1min = reinterpret_cast<float*>(kmin + m);
+  int* ccount = reinterpret_cast<int*>(static_cast<char*>(B[9].p) + 2 * mb + (size_t)m * 4);
+  for (size_t k = 0; k < items.size(); ++k) {  // device addresses of the items' W and records
+    items[k].W = static_cast<const double*>(B[10].p) + offs[k].first;
+    items[k].rec = static_cast<float*>(B[8].p) + offs[k].second;
+  }
+  Stage stg;
+  stg.add(B[1].p, insts);
+  stg.add(B[2].p, gitems);
+  stg.add(B[3].p, uitems);
+  stg.add(B[4].p, gray_ids);
+  stg.add(B[5].p, pre);
+  stg.add(ccount, std::vector<int>(1, prefilled));
+  if (!tcs.empty()) {
+    stg.add(B[11].p, items);
+    stg.add(B[12].p, first);
+  }
+  QB_CUDA(h->hstage.ensure(std::max<size_t>(stg.bytes.size(), 16)));
+  memcpy(h->hstage.p, stg.bytes.data(), stg.bytes.size());
+  int64_t h2d_bytes = (int64_t)(w_used * sizeof(double)) + (int64_t)(wtc_used * sizeof(double));
+  for (auto& c : stg.copies) h2d_bytes += (int64_t)c.bytes;
+  unsigned* tc_err = tcs.empty() ? nullptr : static_cast<unsigned*>(B[13].p);
+  const int64_t d2h_bytes = (int64_t)res_bytes + (tc_err ? (int64_t)sizeof(unsigned) : 0);
+  const double* dW = static_cast<const double*>(B[0].p);
+  const qb::BatchInst* dI = static_cast<const qb::BatchInst*>(B[1].p);
+  qb::BatchCand* dC = static_cast<qb::BatchCand*>(B[5].p);
+  qb::ExactOut* dO = static_cast<qb::ExactOut*>(B[6].p);
+  qb::TcParams P{};
+  size_t sm_tc = 0;
+  if (!tcs.empty()) {
     P.items = static_cast<const qb::TcItem*>(B[11].p);
     P.item_first = static_cast<const uint32_t*>(B[12].p);
     P.n_max = n_tc_max;
     P.err = tc_err;
     const qb::TcSmemLayout L = qb::tc_layout(n_tc_max);
-    const size_t smem = std::max<size_t>(L.total, 120 * 1024) + 1024;
-    QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, smem, h->st>>>(P);
-    ++h->kernels;
+    sm_tc = std::max<size_t>(L.total, 120 * 1024) + 1024;
+    QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
   }
-  QB_CUDA(cudaEventRecord(h->ev[5], h->st));
-  QB_CUDA(cudaEventRecord(h->ev[1], h->st));
-  QB_CUDA(cudaEventRecord(h->ev[2], h->st));
-  if (!gray_ids.empty()) {
-    qb::batch_select_kernel<<<(unsigned)gray_ids.size(), 256, 0, h->st>>>(
-        dI, static_cast<const uint32_t*>(B[4].p), static_cast<const float*>(B[8].p), dC, ccount, cap, p1min, emin,
-        kmin);
-    ++h->kernels;
+  if (any_gray) {
+    QB_CUDA(cudaFuncSetAttribute(qb::batch_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gtab));
+    QB_CUDA(cudaFuncSetAttribute(qb::batch_gray_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gray));
   }
   QB_CUDA(cudaFuncSetAttribute(qb::batch_exact_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_exact));
-  qb::batch_exact_kernel<<<(unsigned)cap, qb::kExactThreads, sm_exact, h->st>>>(dI, dW, dC, ccount, cap, dO, emin);
-  qb::batch_key_kernel<<<(unsigned)std::min<int>((cap + 255) / 256, h->sm_count * 4), 256, 0, h->st>>>(
-      dC, ccount, cap, dO, emin, kmin);
-  h->kernels += 2;
-  QB_CUDA(cudaGetLastError());
-  QB_CUDA(cudaEventRecord(h->ev[3], h->st));
-  QB_CUDA(h->hout.ensure(B[9].cap));
-  QB_CUDA(cudaMemcpyAsync(h->hout.p, B[9].p, 2 * mb + (size_t)m * 4 + sizeof(int), cudaMemcpyDeviceToHost, h->st));
-  h->d2h += (int64_t)(2 * mb + (size_t)m * 4 + sizeof(int));
+  const unsigned key_blocks = (unsigned)std::min<int>((cap + 255) / 256, h->sm_count * 4);
+
+  // the whole device side of the batch: uploads, the six launches, the result copy
+  auto issue = [&](cudaStream_t st, bool timed) -> int {
+    QB_CUDA(cudaMemcpyAsync(B[0].p, Wall, w_used * sizeof(double), cudaMemcpyHostToDevice, st));
+    for (auto& c : stg.copies)
+      QB_CUDA(cudaMemcpyAsync(c.dst, static_cast<unsigned char*>(h->hstage.p) + c.off, c.bytes,
+                              cudaMemcpyHostToDevice, st));
+    QB_CUDA(cudaMemsetAsync(B[9].p, 0xff, 2 * mb, st));
+    if (timed) {
+      QB_CUDA(cudaEventRecord(h->ev[0], st));
+      QB_CUDA(cudaEventRecord(h->ev[4], st));
+    }
+    if (any_gray) {
+      qb::batch_gtab_kernel<<<(unsigned)gitems.size(), 256, sm_gtab, st>>>(
+          dI, static_cast<const qb::BatchItem*>(B[2].p), dW, static_cast<float*>(B[7].p));
+      qb::batch_gray_kernel<<<(unsigned)uitems.size(), qb::kGrayThreads, sm_gray, st>>>(
+          dI, static_cast<const qb::BatchItem*>(B[3].p), dW, static_cast<const float*>(B[7].p),
+          static_cast<float*>(B[8].p));
+      h->kernels += 2;
+    }
+    if (!tcs.empty()) {
+      QB_CUDA(cudaMemcpyAsync(B[10].p, Wtc, wtc_used * sizeof(double), cudaMemcpyHostToDevice, st));
+      QB_CUDA(cudaMemsetAsync(tc_err, 0, 16, st));
+      qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(P);
+      ++h->kernels;
+    }
+    if (timed) {
+      QB_CUDA(cudaEventRecord(h->ev[5], st));
+      QB_CUDA(cudaEventRecord(h->ev[1], st));
+      QB_CUDA(cudaEventRecord(h->ev[2], st));
+    }
+    if (!gray_ids.empty()) {
+      qb::batch_select_kernel<<<(unsigned)gray_ids.size(), 256, 0, st>>>(
+          dI, static_cast<const uint32_t*>(B[4].p), static_cast<const float*>(B[8].p), dC, ccount, cap, p1min,
+          emin, kmin);
+      ++h->kernels;
+    }
+    qb::batch_exact_kernel<<<(unsigned)cap, qb::kExactThreads, sm_exact, st>>>(dI, dW, dC, ccount, cap, dO, emin);
+    qb::batch_key_kernel<<<key_blocks, 256, 0, st>>>(dC, ccount, cap, dO, emin, kmin);
+    h->kernels += 2;
+    QB_CUDA(cudaGetLastError());
+    if (timed) QB_CUDA(cudaEventRecord(h->ev[3], st));
+    QB_CUDA(cudaMemcpyAsync(h->hout.p, B[9].p, res_bytes, cudaMemcpyDeviceToHost, st));
+    if (tc_err)
+      QB_CUDA(cudaMemcpyAsync(static_cast<char*>(h->hout.p) + res_bytes, tc_err, sizeof(unsigned),
+                              cudaMemcpyDeviceToHost, st));
+    return QB_OK;
+  };
+
+  const bool graph = (o->flags & QB_FLAG_GRAPH) != 0;
+  if (graph) {
+    // one graph launch per batch; the graph is captured again whenever the batch's shape, the
+    // options or any buffer address differ from the captured one
+    std::vector<uint64_t> key = {(uint64_t)m, (uint64_t)w_used, (uint64_t)wtc_used, (uint64_t)cap,
+                                 (uint64_t)gitems.size(), (uint64_t)uitems.size(), (uint64_t)gray_ids.size(),
+                                 (uint64_t)first.size(), (uint64_t)sm_gtab, (uint64_t)sm_gray, (uint64_t)sm_exact,
+                                 (uint64_t)sm_tc, (uint64_t)any_gray, (uint64_t)(uintptr_t)Wall,
+                                 (uint64_t)(uintptr_t)h->hstage.p, (uint64_t)(uintptr_t)h->hout.p,
+                                 (uint64_t)(uintptr_t)h->own};
+    for (int k = 0; k < 14; ++k) key.push_back((uint64_t)(uintptr_t)B[k].p);
+    for (auto& c : stg.copies) {
+      key.push_back((uint64_t)(uintptr_t)c.dst);
+      key.push_back((uint64_t)c.off);
+      key.push_back((uint64_t)c.bytes);
+    }
+    if (!h->batch_graph || key != h->batch_graph_key) {
+      if (h->batch_graph) {
+        cudaGraphExecDestroy(h->batch_graph);
+        h->batch_graph = nullptr;
+        h->batch_graph_key.clear();
+      }
+      cudaGraph_t g = nullptr;
+      QB_CUDA(cudaStreamBeginCapture(h->own, cudaStreamCaptureModeThreadLocal));
+      const int k0 = h->kernels;
+      const int irc = issue(h->own, false);
+      const cudaError_t ce = cudaStreamEndCapture(h->own, &g);
+      h->batch_graph_kernels = h->kernels - k0;
+      h->kernels = k0;
+      if (irc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return irc ? irc : cuda_fail(ce);
+      }
+      const cudaError_t ie = cudaGraphInstantiate(&h->batch_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) {
+        h->batch_graph = nullptr;
+        return cuda_fail(ie);
+      }
+      h->batch_graph_key = key;
+    }
+    QB_CUDA(cudaEventRecord(h->ev[0], h->st));
+    QB_CUDA(cudaGraphLaunch(h->batch_graph, h->st));
+    QB_CUDA(cudaEventRecord(h->ev[3], h->st));
+    h->kernels += h->batch_graph_kernels;
+  } else {
+    if ((rc = issue(h->st, true))) return rc;
+  }
+  h->h2d += h2d_bytes;
+  h->d2h += d2h_bytes;
   QB_CUDA(cudaStreamSynchronize(h->st));
   const uint64_t* he = static_cast<const uint64_t*>(h->hout.p);
   const uint64_t* hk = he + m;
@@ -1192,8 +1347,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   const int got = *reinterpret_cast<const int*>(reinterpret_cast<const char*>(h->hout.p) + 2 * mb + (size_t)m * 4);
   if (tc_err) {
     unsigned e = 0;
-    QB_CUDA(cudaMemcpy(&e, tc_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    h->d2h += (int64_t)sizeof(unsigned);
+    memcpy(&e, static_cast<const char*>(h->hout.p) + res_bytes, sizeof(unsigned));
     if (e & qb::kErrTimeout) return QB_ETIMEOUT;
   }
   if (got > cap) {
@@ -1201,9 +1355,14 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     return QB_OK;
   }
   float p1 = 0.f, p2 = 0.f, km = 0.f;
-  QB_CUDA(cudaEventElapsedTime(&p1, h->ev[0], h->ev[1]));
-  QB_CUDA(cudaEventElapsedTime(&p2, h->ev[2], h->ev[3]));
-  QB_CUDA(cudaEventElapsedTime(&km, h->ev[4], h->ev[5]));
+  if (graph) {  // one launch: its whole device time is reported as pass 1 and as the kernel time
+    QB_CUDA(cudaEventElapsedTime(&p1, h->ev[0], h->ev[3]));
+    km = p1;
+  } else {
+    QB_CUDA(cudaEventElapsedTime(&p1, h->ev[0], h->ev[1]));
+    QB_CUDA(cudaEventElapsedTime(&p2, h->ev[2], h->ev[3]));
+    QB_CUDA(cudaEventElapsedTime(&km, h->ev[4], h->ev[5]));
+  }
   for (int j = 0; j < m; ++j) {
     const qb::BatchInst& I = insts[j];
     qb_result& R = r[ids[j]];
@@ -1222,6 +1381,19 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     R.err_bound = I.eps;
     R.states = (int64_t)1 << I.n;
     R.form_used = I.kind == qb::kBatchGray ? QB_FORM_GRAY : (I.kind == qb::kBatchTC ? QB_FORM_TC : QB_FORM_EXACT);
+    const qb_handle::Tuned& T = h->tuned[I.is_int ? 1 : 0][I.n];
+    if (I.kind == qb::kBatchGray) {
+      R.rec_log2 = I.sbits;
+      R.suffix_bits = I.b;
+      R.unit_log2 = I.gubits + I.sbits;
+      R.tuned = (T.gray_b || T.gray_sbits || T.form == QB_FORM_GRAY) ? 1 : 0;
+    } else if (I.kind == qb::kBatchTC) {
+      R.rec_log2 = I.gl;
+      R.suffix_bits = 15;
+      R.tuned = (T.tc_gl || T.form == QB_FORM_TC) ? 1 : 0;
+    } else {
+      R.rec_log2 = I.fbits;
+    }
     R.is_integer = I.is_int;
     R.found = 1;
     R.status = QB_OK;
@@ -1316,14 +1488,16 @@ int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, dou
 
 int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
   if (!h || !form_out || n < 1 || n > qb::kMaxN || dtype_size(dtype) == 0) return QB_EINVAL;
+  const bool is_int = dtype >= QB_I8;
+  qb_handle::Tuned& T = h->tuned[is_int ? 1 : 0][n];
   if (n < 20) {  // the exact form is the only one below 20 variables
-    h->autotuned_form[n] = QB_FORM_EXACT;
+    T = qb_handle::Tuned{};
+    T.form = QB_FORM_EXACT;
     *form_out = QB_FORM_EXACT;
     return QB_OK;
   }
   // a seeded synthetic problem of the dtype's class: integer entries in [-100, 100] for
   // integer dtypes (exact arithmetic), uniform [-1, 1) for float dtypes
-  const bool is_int = dtype >= QB_I8;
   std::vector<double> Q((size_t)n * n);
   uint64_t st = 0x9E3779B97F4A7C15ull ^ (uint64_t)n;
   for (auto& v : Q) {
@@ -1343,15 +1517,43 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
     p.q = Q.data();
   }
   p.ldq = n;
-  // time one shard of at most 2^36 states per form: pass 1 plus candidate re-evaluation
+  // candidates: (form, tc_gl) and (form, gray_b, gray_sbits) around the defaults
+  std::vector<qb_handle::Tuned> cands;
+  {
+    const GrayShape g0 = gray_shape(n);
+    for (int db : {0, -1, 1, -2}) {
+      const int b = g0.b + db;
+      const GrayShape g = gray_shape(n, b);
+      if (g.b != b) continue;  // outside the valid range
+      for (int ds : {0, 1, 2}) {
+        const int sb = std::min(g.a, std::max(5, n - 34)) + ds;
+        if (sb > g.a) continue;
+        qb_handle::Tuned t;
+        t.form = QB_FORM_GRAY;
+        t.gray_b = b;
+        t.gray_sbits = sb;
+        cands.push_back(t);
+      }
+    }
+    if (qb::tc_supported(n)) {
+      const int gl0 = qb::tc_default_gl(n);
+      for (int d = 0; d <= 3; ++d) {
+        if (gl0 + d > n - 15) break;
+        qb_handle::Tuned t;
+        t.form = QB_FORM_TC;
+        t.tc_gl = gl0 + d;
+        cands.push_back(t);
+      }
+    }
+  }
+  // time one shard of at most 2^36 states per candidate: pass 1 plus candidate re-evaluation
   const int shard_bits = std::max(0, n - 36);
   float best_ms = 0.f;
-  int best = QB_FORM_GRAY;
-  const int forms[2] = {QB_FORM_GRAY, QB_FORM_TC};
-  for (int f : forms) {
-    if (f == QB_FORM_TC && !qb::tc_supported(n)) continue;
+  qb_handle::Tuned best{};
+  for (const qb_handle::Tuned& c : cands) {
+    T = c;  // planning reads the handle's entry
     qb_options o{};
-    o.form = f;
+    o.form = c.form;
     o.tie_rule = QB_TIE_QBF;
     o.prefix_bits = -1;
     o.shard_index = 0;
@@ -1360,19 +1562,25 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
     for (int rep = 0; rep < 2; ++rep) {  // warm-up, then the timed call
       double lmin = 0.0;
       int rc = qb_solve_begin(h, &p, &o, &lmin);
-      if (rc) return rc;
+      if (rc) {
+        T = qb_handle::Tuned{};
+        return rc;
+      }
       qb_result r{};
       rc = qb_solve_finish(h, lmin, &r);
-      if (rc) return rc;
+      if (rc) {
+        T = qb_handle::Tuned{};
+        return rc;
+      }
       ms = r.pass1_ms + r.pass2_ms;
     }
     if (best_ms == 0.f || ms < best_ms) {
       best_ms = ms;
-      best = f;
+      best = c;
     }
   }
-  h->autotuned_form[n] = best;
-  *form_out = best;
+  T = best;
+  *form_out = best.form;
   return QB_OK;
 }
 

@@ -109,7 +109,11 @@ inline bool tc_supported(int n) { return n >= 20 && n <= kMaxN; }
 // per-state error bound of the float-digit path (unscaled units)
 inline double tc_error_bound(double abs_sum) { return 256.0 * abs_sum * 5.9604644775390625e-08 + 1e-300; }
 
-inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard_cnt, TcPlan* p) {
+// default record granularity: runs of 32 tiles, at most 2^21 records (8 per block of 2^gl tiles)
+inline int tc_default_gl(int n) { return std::max(5, n - 15 - 18); }
+
+// gl: log2 tiles per record block (0 = tc_default_gl); 5 <= gl <= n - 15
+inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard_cnt, TcPlan* p, int gl = 0) {
   p->n = n;
   p->nt = n - 15;
   p->is_int = is_int;
@@ -124,7 +128,7 @@ inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard
     p->scale = std::ldexp(1.0, e);
     p->eps = tc_error_bound(abs_sum);
   }
-  p->gl = std::max(5, p->nt - 18);  // runs of 32 tiles; at most 2^21 records (8 per block)
+  p->gl = gl >= 5 && gl <= p->nt ? gl : tc_default_gl(n);
   uint64_t groups = 1ull << (p->nt - p->gl);
   unsigned __int128 g = groups;
   uint64_t gb = (uint64_t)(g * (unsigned)shard_idx / (unsigned)shard_cnt);

@@ -140,7 +140,9 @@ class QBF(SolverABC):
         """Solve many independent problems in one batched GPU search (qb_solve_batch) and
         return one Solution per problem, each the one ``solve(problem, **kwargs)`` returns.
         Problems with up to 36 variables share six kernel launches in total; larger ones are
-        solved one by one.  An addition: the reference solves one problem per call."""
+        solved one by one.  ``graph=True`` runs that device work as one CUDA graph launch,
+        captured once and replayed while later batches keep the same shape.  An addition:
+        the reference solves one problem per call."""
         self.check_obsolete_args(**kwargs)
         if "B" in kwargs or "use_mem_GB" in kwargs:  # the split would differ per problem size
             return [QBF().solve(p, **kwargs) for p in problems]
@@ -152,7 +154,8 @@ class QBF(SolverABC):
         Qs = [np.asarray(p.build_Q_matrix(use_gpu=False)) for p in problems]
         self.timer.pick_time("build_Q")
         results = _lib.handle(dev).solve_batch(Qs, form=kwargs.get("form", "auto"), tie_rule="qbf", fixed_bits=0,
-                                               prefix_bits=int(kwargs.get("A", -1)), stream=stream)
+                                               prefix_bits=int(kwargs.get("A", -1)), stream=stream,
+                                               graph=bool(kwargs.get("graph", False)))
         self.timer.pick_time("search")
         out = []
         for problem, Q, res in zip(problems, Qs, results):
@@ -189,7 +192,7 @@ class QBF(SolverABC):
         sol.timer = [(t, lbl) for t, lbl in self.timer.times if lbl != "epoch"]
         sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_min", "err_bound",
                                           "pass1_ms", "pass2_ms", "kernel_ms", "order_key", "kernels",
-                                          "h2d_bytes", "d2h_bytes")}
+                                          "h2d_bytes", "d2h_bytes", "plan")}
         sol.search["split"] = (self.A, self.B)
         return sol
 

@@ -67,6 +67,12 @@ extern "C" {
                                  modulo 2^16), so that the state and the reported best_e_int
                                  are the reference's even where its sums overflow; best_e is
                                  the exact energy of that state (qbf1.py:86-133, 179-289) */
+#define QB_FLAG_GRAPH 4       /* qb_solve_batch: run the batch's device work (uploads, the six
+                                 launches, the result copy) as one CUDA graph launch.  The graph
+                                 is captured on the first call and replayed by later calls whose
+                                 batch has the same shape (sizes, dtype classes, options); any
+                                 other batch is captured anew.  pass1_ms then holds the whole
+                                 graph's device time and pass2_ms is 0 */
 #define QB_FLAG_TEST_STALL 2  /* tests only, QB_FORM_TC: the search kernel's tile walk
                                  publishes nothing, so the kernel's bounded waits run out
                                  (about 2 s); the call returns QB_ETIMEOUT and the handle
@@ -119,6 +125,13 @@ typedef struct qb_result {
   float kernel_ms;        /* device time of the main pass-1 search kernel alone */
   int64_t h2d_bytes;      /* bytes copied host -> device by this call */
   int64_t d2h_bytes;      /* bytes copied device -> host by this call */
+  int32_t rec_log2;       /* record granularity: log2 tiles per record block (QB_FORM_TC),
+                             log2 prefix steps per record (QB_FORM_GRAY), log2 states per
+                             record (QB_FORM_EXACT) */
+  int32_t suffix_bits;    /* QB_FORM_GRAY: suffix bits b of the prefix/suffix split;
+                             QB_FORM_TC: 15 (the 128 x 256 states of a tile); else 0 */
+  int32_t unit_log2;      /* QB_FORM_GRAY: log2 prefix steps per work unit; else 0 */
+  int32_t tuned;          /* 1 when qb_autotune's choice for (n, dtype class) was applied */
 } qb_result;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
@@ -164,12 +177,17 @@ int qb_solve_batch(qb_handle* h, const qb_problem* problems, int32_t count, cons
  * per prefix in update_global_minima (src/qubo_lib/solvers/qbf.py:395-412, 342-351). */
 int qb_prefix_minima(qb_handle* h, const qb_problem* p, int32_t prefix_bits, double* out);
 
-/* Pick the fastest form for problems of n variables and dtype by timing the Gray-code and
- * tensor-core forms (pass 1 + re-evaluation of one shard of at most 2^36 states) on a seeded
- * synthetic problem of the dtype's class on the handle's device; the choice is cached in
- * the handle (per n) and used by QB_FORM_AUTO.  n < 20 always gives QB_FORM_EXACT.
- * *form_out receives the chosen QB_FORM_*.  No reference counterpart beyond
- * QBF.define_chunk_size (src/qubo_lib/solvers/qbf.py:429-466), which picks a split. */
+/* Tune the search for problems of n variables and dtype: times, on a seeded synthetic problem
+ * of the dtype's class (integer or float) on the handle's device, pass 1 + re-evaluation of
+ * one shard of at most 2^36 states for the Gray-code form over its prefix/suffix split and
+ * record granularity, and for the tensor-core form over its record granularity (the
+ * defaults among the candidates), and keeps the fastest (form, parameters) in the handle per
+ * (dtype class, n).  QB_FORM_AUTO then runs that form, and every solve of that class and n
+ * uses the tuned parameters of its form, in qb_solve and in qb_solve_batch; qb_result reports
+ * the parameters used (rec_log2, suffix_bits, unit_log2, tuned).  n < 20 always gives
+ * QB_FORM_EXACT.  *form_out receives the chosen QB_FORM_*.  Generalises
+ * QBF.define_chunk_size (src/qubo_lib/solvers/qbf.py:429-466), which picks a split from
+ * memory size alone. */
 int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out);
 
 /* Result written by qb_solve_noalloc into device memory. */

@@ -122,3 +122,33 @@ def test_batch_tensor_core_members_beyond_exact_digits(cuda_ok):
     for Q, r in zip(Qs, res):
         assert r["form"] == "tc"
         _check(Q, r)
+
+
+def _same_shapes(Qs, seed):
+    """New matrices with the sizes and dtypes of Qs (the same batch shape, other values)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for Q in Qs:
+        n = Q.shape[0]
+        if np.issubdtype(Q.dtype, np.integer):
+            out.append(rng.integers(-9, 10, (n, n)).astype(Q.dtype))
+        else:
+            out.append(rng.standard_normal((n, n)).astype(Q.dtype))
+    return out
+
+
+def test_batch_as_one_graph_launch(cuda_ok):
+    """QB_FLAG_GRAPH: the first batch is captured, a batch of the same shape with other values
+    replays the graph (its new inputs are uploaded by the replay), another shape is captured
+    anew; every answer equals the oracle's and the launch-by-launch run's."""
+    h = _lib.handle(0)
+    Qa = _mixed(31, 48)
+    Qb = _same_shapes(Qa, 32)
+    Qc = _mixed(33, 20)
+    for Qs in (Qa, Qb, Qb, Qc, Qa):
+        g = h.solve_batch(Qs, graph=True)
+        plain = h.solve_batch(Qs)
+        for Q, rg, rp in zip(Qs, g, plain):
+            _check(Q, rg)
+            assert (rg["best_X_int"], rg["best_E"]) == (rp["best_X_int"], rp["best_E"])
+        assert g[0]["kernels"] == plain[0]["kernels"] and g[0]["pass2_ms"] == 0.0
