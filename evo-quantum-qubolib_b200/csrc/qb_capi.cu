@@ -18,6 +18,7 @@
 #include "qb_qbf1.cuh"
 #include "qb_reduce.cuh"
 #include "qb_tc.cuh"
+#include "qb_tc2.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -333,6 +334,8 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
   // tensor-core form
   qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc, T.tc_gl);
   P.tc.stall = (o->flags & QB_FLAG_TEST_STALL) != 0;
+  P.tc.pair = (o->flags & QB_FLAG_TC_ONE_STATE) == 0;
+  if (P.tc.pair && !P.tc.exact) P.tc.eps = qb::tc2_error_bound(P.abs_sum);
   P.geom.kind = qb::kGeomTC;
   P.geom.gl = P.tc.gl;
   P.rec_begin = P.tc.rec_begin;
@@ -428,7 +431,9 @@ int run_pass1(qb_handle* h, Plan& P) {
   int rc = qb::tc_prepare(P.tc, pd, h->tcscratch.p, h->st, &h->kernels);
   if (rc) return rc;
   QB_CUDA(cudaEventRecord(h->ev[4], h->st));
-  rc = qb::tc_launch(P.tc, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st, h->sm_count, &h->kernels);
+  rc = P.tc.pair ? qb::tc2_launch(P.tc, P.tc.gamma, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st,
+                                  h->sm_count, &h->kernels)
+                 : qb::tc_launch(P.tc, static_cast<float*>(h->rec.p), h->tcscratch.p, h->st, h->sm_count, &h->kernels);
   if (rc) return rc;
   QB_CUDA(cudaEventRecord(h->ev[5], h->st));
   return QB_OK;
@@ -527,6 +532,8 @@ int begin_launch(qb_handle* h, const qb_problem* p, const qb_options* o, Plan& P
   if (rc) return rc;
   rc = plan_problem(h, o, P);
   if (rc) return rc;
+  if (P.form == QB_FORM_TC)  // pair form: couplings of variable n-16 with the u variables
+    for (int j = 0; j < 8; ++j) P.tc.gamma[j] = (float)(W[(size_t)(P.n - 16) * P.n + (P.n - 1 - j)] * P.tc.scale);
   rc = upload_W(h, W);
   if (rc) return rc;
   QB_CUDA(h->misc.ensure(64));

@@ -76,6 +76,8 @@ struct TcPlan {
   uint64_t tile_begin = 0, tile_end = 0;  // this shard's Gray tile indices
   uint64_t rec_begin = 0, rec_count = 0, states = 0;
   bool stall = false;      // test hook: the tile walk publishes nothing (waits expire)
+  bool pair = false;       // two states per accumulator (tc_pair_kernel, qb_tc2.cuh)
+  float gamma[8] = {0};    // pair form: scaled W[n-16][n-1-j], j < 8
 };
 
 // one CTA work item: a contiguous run of whole record blocks of one problem

@@ -1,0 +1,457 @@
+// qb_tc2.cuh -- tensor-core form with two states per accumulator (tile pairs), one problem.
+//
+// Same decomposition as qb_tc.cuh (t: tile index in Gray order, y: the 128 MMA rows, u: the
+// 256 MMA columns; E(t, y, u) = R_t(y) + C_t(u) + y^T V u), but the Gray-ordered tiles are
+// taken in pairs (i, i + 1) with i even.  Their tile values t and t' = t ^ 1 differ in t
+// bit 0 (variable n-16) alone, so
+//   E(t', y, u) = R_t'(y) + D(y, u) + s * gamma(u),   D(y, u) = y^T V u + C_t(u)
+//   gamma(u)    = sum_j W[n-16][n-1-j] u_j          (the couplings of variable n-16 with u)
+//   s           = +1 if t bit 0 is 0, else -1       (bit 0 of gray(i) = (i >> 1) & 1)
+// One MMA computes D for tile t; the epilogue reads each accumulator once and derives the
+// partner tile's value with one fma (gamma of the 5 low u bits is a kernel parameter read
+// as a constant operand per register; the 3 high u bits are constant per 32-column chunk
+// and are added to the chunk's minimum).  Every TMEM accumulator thus stands for two
+// states, which halves the MMAs, accumulator round trips and TMEM loads per state: the
+// accumulator round trip (MMA -> commit -> epilogue loads -> release -> next MMA into the
+// stage) over the two 256-column stages is what bounds the one-state-per-accumulator form.
+//
+// Roles, pipelines, records and bounded waits are those of tc_pass1_kernel<false>
+// (qb_tc.cuh), with "tile" replaced by "pair" in the MMA, B-stage and accumulator
+// pipelines: per pair the B producer writes the C_t(u) digits of tile t and the row terms of
+// both tiles.  Records: per block of 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in
+// qb_tc.cuh (kGeomTC); a pair never straddles two blocks.
+//
+// Exactness: for integer Q with sum|Q| <= 2^22, D + s*gamma(u) = y^T V u + C_t'(u) is an
+// integer of magnitude at most sum|Q| (it is the accumulator tile t' would have had), so the
+// fma is exact.  For float Q, gamma in fp32, its partial sums g5, the fma and the chunk
+// offset add at most 8 roundings of 2^-24 relative to sum|Q| (scaled units) to the error
+// bound of the digit contraction; tc2_error_bound() includes them.
+#pragma once
+#include "qb_tc.cuh"
+
+namespace qb {
+
+// per-state error bound of the float-digit pair form (unscaled units)
+inline double tc2_error_bound(double abs_sum) { return 264.0 * abs_sum * 5.9604644775390625e-08 + 1e-300; }
+
+struct Tc2Params {
+  TcParams P;       // n, nt, gl, stall, exact, inv_scale, W, tile_begin, groups, groups_per_cta, rec, err
+  float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
+  float whi[3];     // w_5, w_6, w_7: gamma of u bits 5..7 (scaled W)
+};
+
+#ifdef __CUDACC__
+
+// min over k of (D_k + s * g5[k]) for one 32-column chunk; g5 is read from the parameter
+// space with a constant index per k (a constant operand of the fma)
+__device__ __forceinline__ float min32_shift(const uint32_t* r, const Tc2Params& Q, float s) {
+  float v[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) v[k] = fmaf(Q.g5[k], s, __uint_as_float(r[k]));
+  float m0 = fmin3(v[0], v[1], v[2]);
+  float m1 = fmin3(v[3], v[4], v[5]);
+  float m2 = fmin3(v[6], v[7], v[8]);
+  float m3 = fmin3(v[9], v[10], v[11]);
+  float m4 = fmin3(v[12], v[13], v[14]);
+  float m5 = fmin3(v[15], v[16], v[17]);
+  float m6 = fmin3(v[18], v[19], v[20]);
+  float m7 = fmin3(v[21], v[22], v[23]);
+  float m8 = fmin3(v[24], v[25], v[26]);
+  float m9 = fmin3(v[27], v[28], v[29]);
+  float n0 = fmin3(m0, m1, m2);
+  float n1 = fmin3(m3, m4, m5);
+  float n2 = fmin3(m6, m7, m8);
+  float n3 = fmin3(m9, v[30], v[31]);
+  return fmin3(n0, n1, fminf(n2, n3));
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_constant__ Tc2Params Q) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  const TcParams& P = Q.P;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TcSmemLayout L = tc_layout(P.n);
+  unsigned char* Asm = tc_smem + L.a_off;
+  unsigned char* Bsm = tc_smem + L.b_off;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + L.bar_off);
+  uint64_t* p_full = bars;
+  uint64_t* p_empty = p_full + kTcParamSlots;
+  uint64_t* b_full = p_empty + kTcParamSlots;
+  uint64_t* b_empty = b_full + kTcBStages;
+  uint64_t* acc_full = b_empty + kTcBStages;
+  uint64_t* acc_empty = acc_full + kTcStages;
+  TcSlot* slots = reinterpret_cast<TcSlot*>(tc_smem + L.slot_off);
+  float* EU = reinterpret_cast<float*>(tc_smem + L.eu_off);
+  float* EY = reinterpret_cast<float*>(tc_smem + L.ey_off);
+  float* Rs = reinterpret_cast<float*>(tc_smem + L.rs_off);            // tile t of each pair
+  float* Rs2 = reinterpret_cast<float*>(tc_smem + L.total);            // tile t' of each pair
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + L.misc_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tc_smem + L.misc_off + 4);
+  double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
+  double* Ws = reinterpret_cast<double*>(tc_smem + L.w_off);
+
+  const uint64_t g0 = (uint64_t)blockIdx.x * P.groups_per_cta;
+  if (g0 >= P.groups) return;  // uniform per CTA
+  const uint64_t g1 = min(P.groups, g0 + P.groups_per_cta);
+  const int n = P.n, nt = P.nt, gl = P.gl, exact = P.exact;
+  const uint64_t i_begin = P.tile_begin + (g0 << gl), ntiles = (g1 - g0) << gl;
+  float* rec = P.rec + (g0 << 3);
+  const uint64_t t0 = gray64(i_begin);
+  const float s1 = exact ? 2048.0f : 1.0f;
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcParamSlots; ++s) {
+      mbar_init(&p_full[s], 1);
+      mbar_init(&p_empty[s], 1);
+    }
+    for (int s = 0; s < kTcBStages; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+    }
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], kTcEpiWarps / 2);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
+  for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
+  __syncthreads();
+  for (int e = tid; e < 128 * 16; e += kTcThreads) {
+    int y = e >> 4, k = e & 15;
+    float v;
+    if (k < 14)
+      v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
+    else
+      v = (k & 1) ? s1 : 1.0f;
+    *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
+  }
+  for (int e = tid; e < kTcN * 7; e += kTcThreads) {
+    int u = e / 7, i = e % 7;
+    const double* row = Ws + (n - 9 - i) * n;
+    double v = 0.0;
+    for (int j = 0; j < 8; ++j)
+      if ((u >> j) & 1) v += row[n - 1 - j];
+    __half2 dg = digits((float)v, exact);
+    for (int s = 0; s < kTcBStages; ++s)
+      *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+  }
+  for (int u = tid; u < kTcN; u += kTcThreads) {
+    double e = 0.0;
+    for (int j = 0; j < 8; ++j) {
+      if (!((u >> j) & 1)) continue;
+      const double* row = Ws + (n - 1 - j) * n;
+      e += row[n - 1 - j];
+      for (int j2 = 0; j2 < j; ++j2)
+        if ((u >> j2) & 1) e += row[n - 1 - j2];
+    }
+    EU[u] = (float)e;
+  }
+  for (int y = tid; y < 128; y += kTcThreads) {
+    double e = 0.0;
+    for (int i = 0; i < 7; ++i) {
+      if (!((y >> i) & 1)) continue;
+      const double* row = Ws + (n - 9 - i) * n;
+      e += row[n - 9 - i];
+      for (int i2 = 0; i2 < i; ++i2)
+        if ((y >> i2) & 1) e += row[n - 9 - i2];
+    }
+    EY[y] = (float)e;
+  }
+  for (int e = tid; e < 32 * 16; e += kTcThreads) {
+    const int p = e >> 4, c = e & 15;
+    double v = 0.0;
+    if (c == 15) {
+      for (int k = 0; k < 5; ++k) {
+        if (!((p >> k) & 1)) continue;
+        const double* row = Ws + (n - 16 - k) * n;
+        v += row[n - 16 - k];
+        for (int k2 = 0; k2 < k; ++k2)
+          if ((p >> k2) & 1) v += row[n - 16 - k2];
+      }
+    } else {
+      const int col = c < 8 ? n - 1 - c : n - 9 - (c - 8);
+      for (int k = 0; k < 5; ++k)
+        if ((p >> k) & 1) v += Ws[(n - 16 - k) * n + col];
+    }
+    LO[e] = v;
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t npairs = (uint32_t)(ntiles >> 1);
+
+  bool ok = true;
+  if (warp == 0 && P.stall) {
+    // test hook (QB_FLAG_TEST_STALL): nothing is published, every other wait runs out
+  } else if (warp == 0) {
+    // ------------------------------------------------------------ tile walk (every tile)
+    const int nh = nt - 5;
+    double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) fh[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) gh[k] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) c[k] = 0.0;
+    const uint64_t th0 = t0 >> 5;
+    for (int m = 0; m < nh; ++m) {
+      if (!((th0 >> m) & 1)) continue;
+      const double* row = Ws + (n - 21 - m) * n;
+      eh += row[n - 21 - m];
+      for (int m2 = 0; m2 < m; ++m2)
+        if ((th0 >> m2) & 1) eh += row[n - 21 - m2];
+      if (lane < nh && lane != m) h0 += row[n - 21 - lane];
+      if (lane + 32 < nh && lane + 32 != m) h1 += row[n - 21 - lane - 32];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fh[k] += row[n - 1 - k];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) gh[k] += row[n - 9 - k];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) c[k] += row[n - 16 - k];
+    }
+    for (uint64_t j0 = 0; j0 < ntiles && ok; j0 += 32) {
+      const uint64_t i0 = i_begin + j0;
+      if (j0 > 0) {
+        const int kb = __ffsll((long long)i0) - 1;
+        const int m = kb - 5;
+        const double sg = ((gray64(i0) >> kb) & 1) ? 1.0 : -1.0;
+        const double hm = __shfl_sync(0xffffffffu, m < 32 ? h0 : h1, m & 31);
+        const double* row = Ws + (n - 21 - m) * n;
+        eh += sg * (row[n - 21 - m] + hm);
+        if (lane < nh && lane != m) h0 += sg * row[n - 21 - lane];
+        if (lane + 32 < nh && lane + 32 != m) h1 += sg * row[n - 21 - lane - 32];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) fh[k] += sg * row[n - 1 - k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gh[k] += sg * row[n - 9 - k];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) c[k] += sg * row[n - 16 - k];
+      }
+      const uint64_t j = j0 + (uint64_t)lane;
+      const int tl = (int)(gray64(i0 + (uint64_t)lane) & 31ull);
+      const double* lo = LO + tl * 16;
+      double et = eh + lo[15];
+#pragma unroll
+      for (int k = 0; k < 5; ++k)
+        if ((tl >> k) & 1) et += c[k];
+      const int s = (int)(j % kTcParamSlots);
+      ok = mbar_wait(&p_empty[s], (uint32_t)(((j / kTcParamSlots) & 1) ^ 1), abort_flag);
+      ok = __all_sync(0xffffffffu, ok);
+      if (!ok) break;
+      TcSlot& sl = slots[s];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sl.f[k] = (float)(fh[k] + lo[k]);
+#pragma unroll
+      for (int k = 0; k < 7; ++k) sl.g[k] = (float)(gh[k] + lo[8 + k]);
+      sl.et = (float)et;
+      mbar_arrive(&p_full[s]);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issue (one per pair)
+    if (lane == 0) {
+      const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
+      const uint64_t bdesc0 = umma_desc(smem_u32(Bsm), 128, 256);
+      for (uint32_t p0 = 0; p0 < npairs && ok; p0 += kTcBStages) {
+        const uint32_t pb = (p0 >> 3) & 1u;
+#pragma unroll
+        for (int k = 0; k < kTcBStages; ++k) {
+          const uint32_t as = (uint32_t)k & 1u;
+          ok = mbar_wait(&b_full[k], pb, abort_flag) &&
+               mbar_wait(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
+          if (!ok) break;
+          tc_fence_after();
+          if (p0 + (uint32_t)k >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(k + kTcBStages - kTcStages) % kTcBStages]);
+          tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc0 + (uint64_t)(k * (kTcN * 32 / 16)));
+          tc_commit(&acc_full[as]);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp < 4) {
+    // ------------------------------------------------------------ B producers (per pair)
+    // warp 2 + (p & 1) fills pair p: the C_t(u) digits of tile 2p (rows u = lane + 32 r) and
+    // the row terms of tiles 2p and 2p + 1 (rows y = lane + 32 r)
+    for (uint32_t p = (uint32_t)(warp - 2); p < npairs && ok; p += 2) {
+      const uint32_t ja = 2 * p, jb = ja + 1;
+      const uint32_t sa = ja & (uint32_t)(kTcParamSlots - 1), sb = jb & (uint32_t)(kTcParamSlots - 1);
+      const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+      ok = mbar_wait(&p_full[sa], (ja >> 6) & 1u, abort_flag) && mbar_wait(&p_full[sb], (jb >> 6) & 1u, abort_flag);
+      if (!ok) break;
+      __half2 dg[8];
+      float ra[4], rb[4];
+      {
+        const TcSlot& sl = slots[sa];
+        float s5 = 0.f;
+#pragma unroll
+        for (int jb5 = 0; jb5 < 5; ++jb5)
+          if ((lane >> jb5) & 1) s5 += sl.f[jb5];
+        const float f5 = sl.f[5], f6 = sl.f[6], f7 = sl.f[7];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          float cr = s5;
+          if (r & 1) cr += f5;
+          if (r & 2) cr += f6;
+          if (r & 4) cr += f7;
+          dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const TcSlot& sl = slots[h ? sb : sa];
+        float g5 = sl.et;
+#pragma unroll
+        for (int i = 0; i < 5; ++i)
+          if ((lane >> i) & 1) g5 += sl.g[i];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          float v = g5;
+          if (r & 1) v += sl.g[5];
+          if (r & 2) v += sl.g[6];
+          (h ? rb : ra)[r] = v + EY[lane + 32 * r];
+        }
+      }
+      ok = mbar_wait(&b_empty[bs], ((p >> 3) & 1u) ^ 1u, abort_flag);
+      if (!ok) break;
+      unsigned char* Bst = Bsm + bs * kTcN * 32;
+#pragma unroll
+      for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        Rs[bs * 128 + lane + 32 * r] = ra[r];
+        Rs2[bs * 128 + lane + 32 * r] = rb[r];
+      }
+      fence_proxy_async();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&b_full[bs]);
+        mbar_arrive(&p_empty[sa]);
+        mbar_arrive(&p_empty[sb]);
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3;
+    const int cq = (warp - 4) >> 2;
+    const int y = q * 32 + lane;
+    const float inf = __int_as_float(0x7f800000);
+    float rmin = inf;
+    const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
+    const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+    // gamma of u bits 5..7 for the four 32-column chunks of this half
+    float ghi[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
+    // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
+    uint32_t rec_left = 1u << (gl - 2);
+    uint32_t Jrec = 0;
+    for (uint32_t p = sp; p < npairs && ok; p += 2) {
+      const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+      ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
+      if (!ok) break;
+      const float R1 = Rs[bs * 128 + y];
+      const float R2 = Rs2[bs * 128 + y];
+      // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
+      const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
+      ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
+      if (!ok) break;
+      tc_fence_after();
+      uint32_t ra[32], rb[32];
+      QB_TC_LD32(tbase, ra);
+      QB_TC_LD32(tbase + 32, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      float m1 = fminf(min32(ra), min32(rb));
+      float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
+      QB_TC_LD32(tbase + 64, ra);
+      QB_TC_LD32(tbase + 96, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[sp]);
+      m1 = fminf(m1, fminf(min32(ra), min32(rb)));
+      m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
+      rmin = fmin3(rmin, m1 + R1, m2 + R2);
+      if (--rec_left == 0) {
+        const float wm = warp_min_f(rmin) * P.inv_scale;
+        if (lane == 0) {
+          float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+          if (wm >= 0.f)
+            atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+          else
+            atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+        }
+        ++Jrec;
+        rec_left = 1u << (gl - 2);
+        rmin = inf;
+      }
+    }
+  }
+  if (!ok) {
+    *abort_flag = 1;
+    atomicOr(P.err, kErrTimeout);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+  }
+}
+
+// the pair-form search kernel (one persistent CTA per SM); gamma = couplings of variable
+// n-16 with u bits 0..7, in the units of the scaled W
+inline int tc2_launch(const TcPlan& p, const float* gamma, float* rec, void* scratch, cudaStream_t st, int sms,
+                      int* kernels) {
+  unsigned* err = static_cast<unsigned*>(scratch);
+  double* Wsc = reinterpret_cast<double*>(static_cast<char*>(scratch) + 16);
+  const uint64_t groups = (p.tile_end - p.tile_begin) >> p.gl;
+  if (!groups) return 0;
+  uint64_t ctas = std::min<uint64_t>((uint64_t)sms, groups);
+  uint64_t gpc = (groups + ctas - 1) / ctas;
+  ctas = (groups + gpc - 1) / gpc;
+  if ((gpc << p.gl) >> 32) return 1;
+  Tc2Params Q{};
+  TcParams& P = Q.P;
+  P.n = p.n;
+  P.nt = p.nt;
+  P.gl = p.gl;
+  P.exact = p.exact ? 1 : 0;
+  P.inv_scale = (float)(1.0 / p.scale);
+  P.W = Wsc;
+  P.tile_begin = p.tile_begin;
+  P.groups = groups;
+  P.groups_per_cta = gpc;
+  P.rec = rec;
+  P.err = err;
+  P.stall = p.stall ? 1 : 0;
+  for (int k = 0; k < 32; ++k) {
+    float g = 0.f;
+    for (int j = 0; j < 5; ++j)
+      if ((k >> j) & 1) g += gamma[j];
+    Q.g5[k] = g;
+  }
+  Q.whi[0] = gamma[5];
+  Q.whi[1] = gamma[6];
+  Q.whi[2] = gamma[7];
+  const TcSmemLayout L = tc_layout(p.n);
+  const size_t smem = std::max<size_t>(L.total + kTcBStages * 128 * 4, 120 * 1024) + 1024;
+  if (cudaFuncSetAttribute(tc_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return 4;
+  tc_pair_kernel<<<(unsigned)ctas, kTcThreads, smem, st>>>(Q);
+  ++*kernels;
+  return cudaGetLastError() == cudaSuccess ? 0 : 4;
+}
+#endif
+
+}  // namespace qb
