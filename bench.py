@@ -23,7 +23,10 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-FLOPS_PER_STATE_TC = 32  # one K=16 f16 MMA element per state: 16 multiply-adds
+# algorithmic work per state of the contraction: one K = 16 dot product (7 coupling bits x 2
+# digits + 2 column-term digits) = 16 multiply-adds.  The pair form executes half of it on the
+# tensor cores (one MMA element serves two states) and one fma per derived state.
+FLOPS_PER_STATE_TC = 32
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
 
@@ -36,12 +39,15 @@ def _peaks():
     return 1590.0, 1400.0, "fallback"
 
 
-def _traffic_per_state():
-    """DRAM bytes per state of the tensor-core kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "tc_pass1_kernel.traffic.json")
+def _traffic(kernel: str, states: int):
+    """DRAM bytes (read + write) of one launch of `kernel` over `states` states, from the
+    committed ncu capture profiles/<kernel>.traffic.json: the captured launch's figure when it
+    covered the same number of states, else None."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}.traffic.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return float(d["dram_bytes_per_state"])
+        if int(d.get("states", 0)) == int(states):
+            return float(d["dram_bytes_read"]) + float(d["dram_bytes_write"])
     return None
 
 
@@ -268,7 +274,7 @@ def bench_ours(args):
     peak, peak_sus, peak_kind = _peaks()
     local_states = r0["states"] if world == 1 else r0["states"]
     achieved = local_states * FLOPS_PER_STATE_TC / (kernel_ms * 1e-3) / 1e12
-    tps = _traffic_per_state()
+    kernel_name = "tc_pair_kernel" if form == "tc" else "gray_pass1_kernel"
     line = {
         "metric": "states/s (exhaustive QUBO, exact argmin)",
         "value": states / (ms * 1e-3),
@@ -288,9 +294,12 @@ def bench_ours(args):
         "e2e": {"value": e2e_value, "unit": "states/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(sum(r["kernels"] for r in res)),
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": (tps * local_states if tps is not None else None),
+                     "frac": achieved / peak, "traffic": _traffic(kernel_name, local_states),
+                     "kernel": kernel_name,
                      "peak_kind": f"bf16 dense burst, {peak_kind}", "kernel_ms": kernel_ms,
-                     "flops_per_state": FLOPS_PER_STATE_TC},
+                     "flops_per_state": FLOPS_PER_STATE_TC,
+                     "mma_flops_per_state": FLOPS_PER_STATE_TC / 2 if form == "tc" else 0,
+                     "mma_frac": (achieved / 2 / peak) if form == "tc" else 0.0},
         "gray_form": {"value": states / (gray_ms * 1e-3), "ms_per_step": gray_ms,
                       "kernel_ms": statistics.mean(r["kernel_ms"] for r in gres)},
         "tc_over_gray": (gray_ms / ms),
