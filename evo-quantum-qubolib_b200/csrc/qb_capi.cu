@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -185,32 +186,44 @@ double load_elem(const unsigned char* p, int dt) {
   }
 }
 
+template <class T>
+int host_problem_typed(const qb_problem* p, double* Wout, double* abs_sum) {
+  const int n = p->n;
+  const T* src = static_cast<const T*>(p->q);
+  const size_t ld = (size_t)p->ldq;
+  double s = 0.0;
+  bool bad = false;
+  for (int i = 0; i < n; ++i) {
+    const T* row = src + i * ld;
+    const double d = (double)row[i];
+    bad |= !std::isfinite(d);
+    s += std::fabs(d);
+    Wout[(size_t)i * n + i] = d;
+    for (int j = i + 1; j < n; ++j) {
+      const double a = (double)row[j], b = (double)src[j * ld + i];
+      bad |= !std::isfinite(a) || !std::isfinite(b);
+      s += std::fabs(a) + std::fabs(b);
+      Wout[(size_t)i * n + j] = Wout[(size_t)j * n + i] = a + b;
+    }
+  }
+  if (bad) return QB_EINVAL;
+  *abs_sum = s;
+  return QB_OK;
+}
+
 // Q in host memory (any dtype) -> W (n x n doubles, written to Wout) and sum |Q_ij|, without
 // intermediate copies (the batched search packs thousands of these).
 int load_host_problem_into(const qb_problem* p, double* Wout, double* abs_sum, bool* is_int) {
-  const int n = p->n;
-  const int es = dtype_size(p->dtype);
-  const unsigned char* src = static_cast<const unsigned char*>(p->q);
-  const size_t ld = (size_t)p->ldq * es;
-  double s = 0.0;
-  for (int i = 0; i < n; ++i) {
-    for (int j = i; j < n; ++j) {
-      const double a = load_elem(src + i * ld + (size_t)j * es, p->dtype);
-      if (i == j) {
-        if (!std::isfinite(a)) return QB_EINVAL;
-        s += std::fabs(a);
-        Wout[(size_t)i * n + i] = a;
-      } else {
-        const double b = load_elem(src + j * ld + (size_t)i * es, p->dtype);
-        if (!std::isfinite(a) || !std::isfinite(b)) return QB_EINVAL;
-        s += std::fabs(a) + std::fabs(b);
-        Wout[(size_t)i * n + j] = Wout[(size_t)j * n + i] = a + b;
-      }
-    }
-  }
-  *abs_sum = s;
   *is_int = p->dtype >= QB_I8;
-  return QB_OK;
+  switch (p->dtype) {
+    case QB_F32: return host_problem_typed<float>(p, Wout, abs_sum);
+    case QB_F64: return host_problem_typed<double>(p, Wout, abs_sum);
+    case QB_I8: return host_problem_typed<int8_t>(p, Wout, abs_sum);
+    case QB_I16: return host_problem_typed<int16_t>(p, Wout, abs_sum);
+    case QB_I32: return host_problem_typed<int32_t>(p, Wout, abs_sum);
+    case QB_I64: return host_problem_typed<int64_t>(p, Wout, abs_sum);
+    default: return QB_EINVAL;
+  }
 }
 
 // Q (any dtype, host or device) -> W (n x n doubles) and sum |Q_ij|.
@@ -1003,6 +1016,24 @@ constexpr int kBatchMaxN = 36;            // larger problems are solved one by o
 constexpr int kBatchTcMinN = 24;          // from here on the tensor-core form (>= 512 tiles)
 constexpr uint64_t kBatchGtabChunk = 1024;  // G-table steps per CTA
 
+// fn(lo, hi) over [0, count) split into contiguous ranges on up to 16 threads (one thread for
+// small counts)
+template <class F>
+void parallel_ranges(int count, F fn) {
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int nt = std::max(1, std::min({16, hw, count / 64}));
+  if (nt <= 1) {
+    fn(0, count);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) {
+    const int lo = (int)((int64_t)count * t / nt), hi = (int)((int64_t)count * (t + 1) / nt);
+    th.emplace_back([=]() { fn(lo, hi); });
+  }
+  for (auto& x : th) x.join();
+}
+
 // Host -> device copies of qb_solve_batch's small arrays, staged in one pinned buffer so that
 // every copy reads from a stable address (a captured graph replays the same copies)
 struct Stage {
@@ -1060,21 +1091,45 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   int n_tc_max = 0;
   bool any_gray = false;
   const bool tc_allowed = o->form == QB_FORM_AUTO || o->form == QB_FORM_TC;
+  // every problem's W and sum |Q| (host matrices converted on several threads; a device
+  // matrix is copied back on the handle's stream first)
+  std::vector<uint64_t> w_offs(m);
+  std::vector<double> sums(m, 0.0);
+  std::vector<char> ints(m, 0);
+  std::vector<int> rcs(m, QB_OK);
+  {
+    uint64_t off = 0;
+    for (int j = 0; j < m; ++j) {
+      w_offs[j] = off;
+      off += (uint64_t)problems[ids[j]].n * problems[ids[j]].n;
+    }
+    for (int j = 0; j < m; ++j) {
+      const qb_problem* p = &problems[ids[j]];
+      if (!p->q_on_device) continue;
+      std::vector<double> Wv;
+      bool ii = false;
+      rcs[j] = load_problem(h, p, Wv, &sums[j], &ii);
+      ints[j] = ii;
+      if (!rcs[j]) memcpy(Wall + w_offs[j], Wv.data(), Wv.size() * sizeof(double));
+    }
+    auto convert = [&](int j0, int j1) {
+      for (int j = j0; j < j1; ++j) {
+        const qb_problem* p = &problems[ids[j]];
+        if (p->q_on_device) continue;
+        bool ii = false;
+        rcs[j] = load_host_problem_into(p, Wall + w_offs[j], &sums[j], &ii);
+        ints[j] = ii;
+      }
+    };
+    parallel_ranges(m, convert);
+  }
+  std::vector<std::pair<int, double>> tc_scale;  // (problem, scale) of the tensor-core problems
   for (int j = 0; j < m; ++j) {
     const qb_problem* p = &problems[ids[j]];
     const int n = p->n;
-    double* W = Wall + w_used;
-    double abs_sum = 0.0;
-    bool is_int = false;
-    int rc;
-    if (p->q_on_device) {
-      std::vector<double> Wv;
-      rc = load_problem(h, p, Wv, &abs_sum, &is_int);
-      if (!rc) memcpy(W, Wv.data(), Wv.size() * sizeof(double));
-    } else {
-      rc = load_host_problem_into(p, W, &abs_sum, &is_int);
-    }
-    if (rc) return rc;
+    const double abs_sum = sums[j];
+    const bool is_int = ints[j] != 0;
+    if (rcs[j]) return rcs[j];
     if (abs_sum >= kTwo53) return QB_ERANGE;
     qb::BatchInst& I = insts[j];
     memset(&I, 0, sizeof(I));
@@ -1084,7 +1139,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     I.A = o->prefix_bits < 0 ? n - std::min(n, 20) : o->prefix_bits;
     if (I.A > n) return QB_EINVAL;
     I.B = n - I.A;
-    I.w_off = w_used;
+    I.w_off = w_offs[j];
     w_used += (uint64_t)n * n;
     int free_bits;
     const qb_handle::Tuned& T = h->tuned[is_int ? 1 : 0][n];
@@ -1103,7 +1158,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
       I.rec_off = rec_total;
       rec_total += I.nrec;
       tcs.emplace_back(j, wtc_used);
-      for (uint64_t e = 0; e < (uint64_t)n * n; ++e) Wtc[wtc_used + e] = W[e] * tp.scale;
+      tc_scale.emplace_back(j, tp.scale);
       wtc_used += (uint64_t)n * n;
       gray_ids.push_back((uint32_t)j);
       n_tc_max = std::max(n_tc_max, n);
@@ -1140,6 +1195,17 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     }
     sm_exact = std::max(sm_exact, qb::exact_smem_bytes(n, free_bits));
   }
+  // the tensor-core problems' W scaled into their own block (several threads)
+  parallel_ranges((int)tcs.size(), [&](int k0, int k1) {
+    for (int k = k0; k < k1; ++k) {
+      const int j = tcs[k].first;
+      const uint64_t nn = (uint64_t)insts[j].n * insts[j].n;
+      const double sc = tc_scale[k].second;
+      const double* W = Wall + w_offs[j];
+      double* dst = Wtc + tcs[k].second;
+      for (uint64_t e = 0; e < nn; ++e) dst[e] = W[e] * sc;
+    }
+  });
   // candidate list: the small problems' records first, then room for the Gray problems'
   const int prefilled = (int)pre.size();
   const int cap = prefilled + std::max(4096, 8 * (int)gray_ids.size());

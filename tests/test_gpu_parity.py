@@ -200,9 +200,10 @@ def test_tensor_core_pair_and_one_state_forms(cuda_ok, n):
             r = h.solve(Q, form="tc", tc_one_state=one)
             assert r["form"] == "tc"
             _check(Q, _as_sol(r), ref)
-        mins = [h.solve_begin(Q, form="tc", shard_index=s, shard_count=3) for s in range(3)]
-        for s in range(3):
-            h.solve_finish(mins[s], n)
+        mins = []
+        for s in range(3):  # one pending two-phase solve per handle: begin, then finish
+            mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3))
+            h.solve_finish(mins[-1], n)
         outs = []
         for s in range(3):
             h.solve_begin(Q, form="tc", shard_index=s, shard_count=3)

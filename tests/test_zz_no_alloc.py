@@ -159,8 +159,9 @@ def test_rejected_input(torch_cuda):
 
 
 def test_too_many_candidates(torch_cuda):
-    """Float Q = 0: every record ties with the minimum, far more than the 4096 that fit."""
-    r = _status(torch_cuda, np.zeros((24, 24)), False)
+    """Float Q = 0 at n = 28: every one of the 8192 records ties with the minimum, more than
+    the 4096 that fit."""
+    r = _status(torch_cuda, np.zeros((28, 28)), False)
     assert r.status == _lib.QB_EOVERFLOW and r.candidates > 4096
 
 
