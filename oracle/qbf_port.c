@@ -112,38 +112,78 @@ static int qbf_solve_##SUF(int n, const double* Q, int A, int corr, oq_result* r
       row[s] = row[s & (s - 1)] + w;                                                  \
     }                                                                                 \
   }                                                                                   \
-  memcpy(chunk, diag_bb, M * sizeof(T));                                              \
-  double glob_e = 0.0; uint64_t glob_pref = 0, glob_x = 0;                            \
-  uint64_t prev = 0;                                                                  \
+  /* The prefix loop runs in contiguous ranges of Gray steps on several threads.  A range   \
+   * starts at a multiple of the correction period, where the sequential loop has just     \
+   * recomputed the running vector from scratch (do_correction): a range that starts by     \
+   * the same recomputation repeats the sequential arithmetic bit for bit.  Each range keeps \
+   * its first strict minimum; the ranges are combined in step order (the earliest wins     \
+   * ties), then against the loop's initial best (E = 0 at state 0).                       \
+   * Without periodic correction the loop stays on one thread. */                         \
   uint64_t steps = (uint64_t)1 << A;                                                  \
-  for (uint64_t i = 0; i < steps; ++i) {                                              \
-    uint64_t gray = i ^ (i >> 1);                                                     \
-    if (i > 0) {                                                                      \
-      int bit = __builtin_ctzll(gray ^ prev);                                         \
-      const T* row = abba + (size_t)(A - 1 - bit) * M;                                \
-      if (gray > prev) { for (size_t s = 0; s < M; ++s) chunk[s] += row[s]; }         \
-      else             { for (size_t s = 0; s < M; ++s) chunk[s] -= row[s]; }         \
-      if (corr > 0 && (i + 1) % (uint64_t)corr == 0) { /* do_correction */            \
-        memcpy(chunk, diag_bb, M * sizeof(T));                                        \
-        for (int k = 0; k < A; ++k)                                                   \
-          if ((gray >> (A - 1 - k)) & 1) {                                            \
-            const T* rk = abba + (size_t)k * M;                                       \
-            for (size_t s = 0; s < M; ++s) chunk[s] += rk[s];                         \
-          }                                                                           \
-      }                                                                               \
-    }                                                                                 \
-    prev = gray;                                                                      \
-    size_t x = 0; T best = chunk[0];                                                  \
-    for (size_t s = 1; s < M; ++s) if (chunk[s] < best) { best = chunk[s]; x = s; }   \
-    double pe = 0.0;  /* prefix_E = b^T Q_0A b in FP64 (qbf.py:409) */                \
-    for (int a = 0; a < A; ++a) {                                                     \
-      if (!((gray >> (A - 1 - a)) & 1)) continue;                                     \
-      for (int c = 0; c < A; ++c)                                                     \
-        if ((gray >> (A - 1 - c)) & 1) pe += Q[(size_t)a * n + c];                    \
-    }                                                                                 \
-    double cand = (double)best + pe;                                                  \
-    if (cand < glob_e) { glob_e = cand; glob_pref = gray; glob_x = x; }               \
+  uint64_t per = steps;                                                               \
+  int nth = 1;                                                                        \
+  if (corr > 0 && steps >= 2 * (uint64_t)corr) {                                      \
+    nth = omp_get_max_threads();                                                      \
+    uint64_t blocks = steps / (uint64_t)corr;                                         \
+    if ((uint64_t)nth > blocks) nth = (int)blocks;                                    \
+    per = ((blocks + (uint64_t)nth - 1) / (uint64_t)nth) * (uint64_t)corr;            \
+    nth = (int)((steps + per - 1) / per);                                             \
   }                                                                                   \
+  double* r_e = (double*)malloc((size_t)nth * sizeof(double));                        \
+  uint64_t* r_p = (uint64_t*)malloc((size_t)nth * sizeof(uint64_t));                  \
+  uint64_t* r_x = (uint64_t*)malloc((size_t)nth * sizeof(uint64_t));                  \
+  int fail = 0;                                                                       \
+  _Pragma("omp parallel for schedule(static, 1) num_threads(nth)")                    \
+  for (int t = 0; t < nth; ++t) {                                                     \
+    uint64_t i0 = (uint64_t)t * per, i1 = i0 + per < steps ? i0 + per : steps;        \
+    T* ch = t == 0 ? chunk : (T*)malloc(M * sizeof(T));                               \
+    r_e[t] = INFINITY; r_p[t] = 0; r_x[t] = 0;                                        \
+    if (!ch) { fail = 1; continue; }                                                  \
+    memcpy(ch, diag_bb, M * sizeof(T));                                               \
+    uint64_t prev = 0;                                                                \
+    if (i0 > 0) { /* the state of step i0 - 1 after its correction */                 \
+      prev = (i0 - 1) ^ ((i0 - 1) >> 1);                                              \
+      for (int k = 0; k < A; ++k)                                                     \
+        if ((prev >> (A - 1 - k)) & 1) {                                              \
+          const T* rk = abba + (size_t)k * M;                                         \
+          for (size_t s = 0; s < M; ++s) ch[s] += rk[s];                              \
+        }                                                                             \
+    }                                                                                 \
+    for (uint64_t i = i0; i < i1; ++i) {                                              \
+      uint64_t gray = i ^ (i >> 1);                                                   \
+      if (i > 0) {                                                                    \
+        int bit = __builtin_ctzll(gray ^ prev);                                       \
+        const T* row = abba + (size_t)(A - 1 - bit) * M;                              \
+        if (gray > prev) { for (size_t s = 0; s < M; ++s) ch[s] += row[s]; }          \
+        else             { for (size_t s = 0; s < M; ++s) ch[s] -= row[s]; }          \
+        if (corr > 0 && (i + 1) % (uint64_t)corr == 0) { /* do_correction */          \
+          memcpy(ch, diag_bb, M * sizeof(T));                                         \
+          for (int k = 0; k < A; ++k)                                                 \
+            if ((gray >> (A - 1 - k)) & 1) {                                          \
+              const T* rk = abba + (size_t)k * M;                                     \
+              for (size_t s = 0; s < M; ++s) ch[s] += rk[s];                          \
+            }                                                                         \
+        }                                                                             \
+      }                                                                               \
+      prev = gray;                                                                    \
+      size_t x = 0; T best = ch[0];                                                   \
+      for (size_t s = 1; s < M; ++s) if (ch[s] < best) { best = ch[s]; x = s; }       \
+      double pe = 0.0;  /* prefix_E = b^T Q_0A b in FP64 (qbf.py:409) */              \
+      for (int a = 0; a < A; ++a) {                                                   \
+        if (!((gray >> (A - 1 - a)) & 1)) continue;                                   \
+        for (int c = 0; c < A; ++c)                                                   \
+          if ((gray >> (A - 1 - c)) & 1) pe += Q[(size_t)a * n + c];                  \
+      }                                                                               \
+      double cand = (double)best + pe;                                                \
+      if (cand < r_e[t]) { r_e[t] = cand; r_p[t] = gray; r_x[t] = x; }                \
+    }                                                                                 \
+    if (t != 0) free(ch);                                                             \
+  }                                                                                   \
+  double glob_e = 0.0; uint64_t glob_pref = 0, glob_x = 0;                            \
+  for (int t = 0; t < nth; ++t)                                                       \
+    if (r_e[t] < glob_e) { glob_e = r_e[t]; glob_pref = r_p[t]; glob_x = r_x[t]; }    \
+  free(r_e); free(r_p); free(r_x);                                                    \
+  if (fail) { free(diag_bb); free(abba); free(chunk); return -2; }                    \
   r->best_e = glob_e;                                                                 \
   r->best_e_int = (int64_t)llround(glob_e);                                           \
   r->glob_pref = glob_pref; r->glob_x = glob_x;                                       \
