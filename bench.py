@@ -24,8 +24,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic work per state of the contraction: one K = 16 dot product (7 coupling bits x 2
-# digits + 2 column-term digits) = 16 multiply-adds.  The pair form executes half of it on the
-# tensor cores (one MMA element serves two states) and one fma per derived state.
+# digits + 2 column-term digits) = 16 multiply-adds, one MMA accumulator element per state
 FLOPS_PER_STATE_TC = 32
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
@@ -212,16 +211,16 @@ def bench_ours(args):
     h = _lib.handle(local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
 
-    def step(form):
+    def step(form, **kw):
         if world == 1:
             return h.solve_device(Qd.data_ptr(), n, Q.dtype, form=form, tie_rule="qbf", prefix_bits=-1,
-                                  stream=stream.cuda_stream)
+                                  stream=stream.cuda_stream, **kw)
         from qubo_b200.distributed import solve_sharded
         return solve_sharded(Q, form=form, device=local, Q_device_ptr=Qd.data_ptr())
 
-    def timed(form, steps, warmup):
+    def timed(form, steps, warmup, **kw):
         for _ in range(warmup):
-            step(form)
+            step(form, **kw)
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
@@ -230,7 +229,7 @@ def bench_ours(args):
         for k in range(steps):
             flush.zero_()
             ev[k][0].record(stream)
-            res.append(step(form))
+            res.append(step(form, **kw))
             ev[k][1].record(stream)
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in ev)
@@ -241,10 +240,13 @@ def bench_ours(args):
         return float(t.item()) / steps, res
 
     form = args.form
+    if form == "tc_pair":
+        raise SystemExit("--form tc_pair is a profiling case option (--case cfg2 or n36); the headline times it beside tc")
     with ClockSampler(local) as clk:
         ms, res = timed(form, args.steps, args.warmup)
     clocks = clk.summary()
     gray_ms, gres = timed("gray", max(3, args.steps // 2), 3)
+    pair_ms, pres = timed("tc", max(3, args.steps // 2), 3, tc_pair=True) if form == "tc" else (None, [])
     r0 = res[-1]
     # e2e: the public API with a host-resident problem, H2D and D2H inside the timed region
     prob = Just_Q(Q)
@@ -274,7 +276,7 @@ def bench_ours(args):
     peak, peak_sus, peak_kind = _peaks()
     local_states = r0["states"] if world == 1 else r0["states"]
     achieved = local_states * FLOPS_PER_STATE_TC / (kernel_ms * 1e-3) / 1e12
-    kernel_name = "tc_pair_kernel" if form == "tc" else "gray_pass1_kernel"
+    kernel_name = "tc_pass1_kernel" if form == "tc" else "gray_pass1_kernel"
     line = {
         "metric": "states/s (exhaustive QUBO, exact argmin)",
         "value": states / (ms * 1e-3),
@@ -297,12 +299,12 @@ def bench_ours(args):
                      "frac": achieved / peak, "traffic": _traffic(kernel_name, local_states),
                      "kernel": kernel_name,
                      "peak_kind": f"bf16 dense burst, {peak_kind}", "kernel_ms": kernel_ms,
-                     "flops_per_state": FLOPS_PER_STATE_TC,
-                     "mma_flops_per_state": FLOPS_PER_STATE_TC / 2 if form == "tc" else 0,
-                     "mma_frac": (achieved / 2 / peak) if form == "tc" else 0.0},
+                     "flops_per_state": FLOPS_PER_STATE_TC},
         "gray_form": {"value": states / (gray_ms * 1e-3), "ms_per_step": gray_ms,
                       "kernel_ms": statistics.mean(r["kernel_ms"] for r in gres)},
         "tc_over_gray": (gray_ms / ms),
+        "tc_pair_form": ({"ms_per_step": pair_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in pres)}
+                         if pres else None),
         "clocks": clocks,
     }
     if rank == 0 and world == 1:
@@ -317,20 +319,23 @@ def bench_ours(args):
 
 
 def bench_case(args):
-    """A small profiling case: the 32-variable integer QUBO (RandomQUBO seed 0, entries in
-    [-100, 100], symmetric int16), solved `steps` times with one form; prints one line per
-    solve.  Used for ncu captures of a single kernel (a few MB on the device)."""
+    """Profiling cases, solved `steps` times with one form, one line per solve: cfg2 = the
+    32-variable integer QUBO (RandomQUBO seed 0, entries in [-100, 100], symmetric int16);
+    n36 = the headline 36-variable TSP QUBO.  Used for ncu captures of a single kernel (a few
+    MB on the device).  --form tc_pair runs the tensor-core pair form."""
     import torch
     import qubo_b200  # noqa: F401
     from qubo_b200 import _lib, configs
     torch.cuda.set_device(0)
-    Q = configs.random_i16_n32()
+    Q = configs.random_i16_n32() if args.case == "cfg2" else configs.tsp6_int()
+    name = "random_i16_n32" if args.case == "cfg2" else "tsp6_int_n36"
     h = _lib.handle(0)
     stream = torch.cuda.current_stream(0).cuda_stream
+    form, kw = (("tc", {"tc_pair": True}) if args.form == "tc_pair" else (args.form, {}))
     for k in range(args.warmup + args.steps):
-        r = h.solve(Q, form=args.form, stream=stream)
+        r = h.solve(Q, form=form, stream=stream, **kw)
         if k >= args.warmup:
-            print(json.dumps({"case": "random_i16_n32", "form": r["form"], "best_E": r["best_E"],
+            print(json.dumps({"case": name, "form": args.form, "best_E": r["best_E"], "states": r["states"],
                               "kernel_ms": r["kernel_ms"], "pass1_ms": r["pass1_ms"], "pass2_ms": r["pass2_ms"]}),
                   flush=True)
 
@@ -431,9 +436,9 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto"])
-    ap.add_argument("--case", default=None, choices=["cfg2", "batch"],
-                    help="cfg2: small profiling case; batch: the 4096-instance batch line")
+    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto", "tc_pair"])
+    ap.add_argument("--case", default=None, choices=["cfg2", "n36", "batch"],
+                    help="cfg2, n36: profiling cases (one line per solve); batch: the 4096-instance batch line")
     args = ap.parse_args()
     if args.case == "batch":
         bench_batch(args)

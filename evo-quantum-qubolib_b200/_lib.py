@@ -22,7 +22,7 @@ FORM_NAMES[4] = "qb_f1_int16"
 QB_FLAG_INT16_WRAP = 1
 QB_FLAG_TEST_STALL = 2
 QB_FLAG_GRAPH = 4
-QB_FLAG_TC_ONE_STATE = 8
+QB_FLAG_TC_PAIR = 8
 TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
 
 _DTYPES = {
@@ -153,12 +153,12 @@ class Handle:
     @staticmethod
     def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
                 max_candidates=0, stream=None, int16_wrap=False, flags=0, graph=False,
-                tc_one_state=False) -> QbOptions:
+                tc_pair=False) -> QbOptions:
         return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
                          prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
                          max_candidates=int(max_candidates),
                          flags=int(flags) | (QB_FLAG_INT16_WRAP if int16_wrap else 0) | (QB_FLAG_GRAPH if graph else 0) |
-                         (QB_FLAG_TC_ONE_STATE if tc_one_state else 0),
+                         (QB_FLAG_TC_PAIR if tc_pair else 0),
                          stream=stream)
 
     def solve(self, Q: np.ndarray, **opts) -> dict:

@@ -145,6 +145,7 @@ struct qb_handle_s {
   struct Tuned {
     int form = 0;
     int tc_gl = 0;
+    int tc_pair = 0;  // tensor-core pair form (two states per accumulator)
     int gray_b = 0, gray_sbits = 0;
   };
   Tuned tuned[2][qb::kMaxN + 1];
@@ -347,7 +348,7 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
   // tensor-core form
   qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc, T.tc_gl);
   P.tc.stall = (o->flags & QB_FLAG_TEST_STALL) != 0;
-  P.tc.pair = (o->flags & QB_FLAG_TC_ONE_STATE) == 0;
+  P.tc.pair = (o->flags & QB_FLAG_TC_PAIR) != 0 || T.tc_pair;
   if (P.tc.pair && !P.tc.exact) P.tc.eps = qb::tc2_error_bound(P.abs_sum);
   P.geom.kind = qb::kGeomTC;
   P.geom.gl = P.tc.gl;
@@ -1610,13 +1611,15 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
     }
     if (qb::tc_supported(n)) {
       const int gl0 = qb::tc_default_gl(n);
-      for (int d = 0; d <= 3; ++d) {
-        if (gl0 + d > n - 15) break;
-        qb_handle::Tuned t;
-        t.form = QB_FORM_TC;
-        t.tc_gl = gl0 + d;
-        cands.push_back(t);
-      }
+      for (int pair = 0; pair < 2; ++pair)
+        for (int d = 0; d <= 3; ++d) {
+          if (gl0 + d > n - 15) break;
+          qb_handle::Tuned t;
+          t.form = QB_FORM_TC;
+          t.tc_gl = gl0 + d;
+          t.tc_pair = pair;
+          cands.push_back(t);
+        }
     }
   }
   // time one shard of at most 2^36 states per candidate: pass 1 plus candidate re-evaluation

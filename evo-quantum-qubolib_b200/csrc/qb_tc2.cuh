@@ -11,15 +11,14 @@
 // partner tile's value with one fma (gamma of the 5 low u bits is a kernel parameter read
 // as a constant operand per register; the 3 high u bits are constant per 32-column chunk
 // and are added to the chunk's minimum).  Every TMEM accumulator thus stands for two
-// states, which halves the MMAs, accumulator round trips and TMEM loads per state: the
-// accumulator round trip (MMA -> commit -> epilogue loads -> release -> next MMA into the
-// stage) over the two 256-column stages is what bounds the one-state-per-accumulator form.
+// states, which halves the MMAs, accumulator round trips and TMEM loads per state, at the
+// price of one fma per derived state in the epilogue.  Measured on B200 (n = 36): 3.9-4.1 ms
+// per 2^36 states, the same as the one-state kernel (3.94 ms); qb_autotune times both.
 //
 // Roles, pipelines, records and bounded waits are those of tc_pass1_kernel<false>
 // (qb_tc.cuh), with "tile" replaced by "pair" in the MMA, B-stage and accumulator
 // pipelines: per pair the B producer writes the C_t(u) digits of tile t and the row terms of
-// both tiles.  The epilogue differs: all 16 epilogue warps read every pair (a lane quarter
-// and a 64-column quarter each, one load round) and release the stage before computing.  Records: per block of 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in
+// both tiles.  Records: per block of 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in
 // qb_tc.cuh (kGeomTC); a pair never straddles two blocks.
 //
 // Exactness: for integer Q with sum|Q| <= 2^22, D + s*gamma(u) = y^T V u + C_t'(u) is an
@@ -37,18 +36,27 @@ inline double tc2_error_bound(double abs_sum) { return 264.0 * abs_sum * 5.96046
 
 struct Tc2Params {
   TcParams P;       // n, nt, gl, stall, exact, inv_scale, W, tile_begin, groups, groups_per_cta, rec, err
-  float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
+  alignas(8) float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
   float whi[3];     // w_5, w_6, w_7: gamma of u bits 5..7 (scaled W)
 };
 
 #ifdef __CUDACC__
 
-// min over k of (D_k + s * g5[k]) for one 32-column chunk; g5 is read from the parameter
-// space with a constant index per k (a constant operand of the fma)
+// min over k of (D_k + s * g5[k]) for one 32-column chunk, two registers per packed fma
+// (fma.rn.f32x2: the same rounding as two scalar fmas); g5 pairs are read from the parameter
+// space with a constant index
 __device__ __forceinline__ float min32_shift(const uint32_t* r, const Tc2Params& Q, float s) {
   float v[32];
+  const uint64_t ss = ((uint64_t)__float_as_uint(s) << 32) | __float_as_uint(s);
 #pragma unroll
-  for (int k = 0; k < 32; ++k) v[k] = fmaf(Q.g5[k], s, __uint_as_float(r[k]));
+  for (int k = 0; k < 16; ++k) {
+    const uint64_t g = *reinterpret_cast<const uint64_t*>(&Q.g5[2 * k]);
+    const uint64_t d = ((uint64_t)r[2 * k + 1] << 32) | r[2 * k];
+    uint64_t o;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(o) : "l"(g), "l"(ss), "l"(d));
+    v[2 * k] = __uint_as_float((uint32_t)o);
+    v[2 * k + 1] = __uint_as_float((uint32_t)(o >> 32));
+  }
   float m0 = fmin3(v[0], v[1], v[2]);
   float m1 = fmin3(v[3], v[4], v[5]);
   float m2 = fmin3(v[6], v[7], v[8]);
@@ -110,7 +118,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
     }
     for (int s = 0; s < kTcStages; ++s) {
       mbar_init(&acc_full[s], 1);
-      mbar_init(&acc_empty[s], kTcEpiWarps);  // every epilogue warp reads every pair
+      mbar_init(&acc_empty[s], kTcEpiWarps / 2);
     }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -338,49 +346,52 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
     }
   } else {
     // ------------------------------------------------------------ epilogue
-    // Every epilogue warp reads every pair: warp w takes TMEM lanes 32*(w%4) .. +31 and the
-    // column quarter cq = (w-4)/4 (64 columns: u bit 7 = cq >> 1, u bit 6 = cq & 1) in one
-    // load round, and releases the accumulator stage before its arithmetic, so a stage is
-    // held only for its loads.
     const int q = warp & 3;
     const int cq = (warp - 4) >> 2;
-    const uint32_t hh = (uint32_t)cq >> 1;  // column half: u bit 7 (record geometry)
     const int y = q * 32 + lane;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
-    const uint32_t lbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)cq * 64u;
-    // gamma of u bits 5..7 for the two 32-column chunks of this quarter
-    const float ghi0 = ((cq & 1) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
-    const float ghi1 = ghi0 + Q.whi[0];
-    // records every 2^gl tiles = 2^(gl-1) pairs
-    uint32_t rec_left = 1u << (gl - 1);
+    const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
+    const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+    // gamma of u bits 5..7 for the four 32-column chunks of this half
+    float ghi[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
+    // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
+    uint32_t rec_left = 1u << (gl - 2);
     uint32_t Jrec = 0;
-    for (uint32_t p = 0; p < npairs && ok; ++p) {
+    for (uint32_t p = sp; p < npairs && ok; p += 2) {
       const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-      const uint32_t as = p & 1u;
       ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
       if (!ok) break;
       const float R1 = Rs[bs * 128 + y];
       const float R2 = Rs2[bs * 128 + y];
       // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
       const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
-      ok = mbar_wait(&acc_full[as], (p >> 1) & 1u, abort_flag);
+      ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
       if (!ok) break;
       tc_fence_after();
       uint32_t ra[32], rb[32];
-      QB_TC_LD32(lbase + as * (uint32_t)kTcN, ra);
-      QB_TC_LD32(lbase + as * (uint32_t)kTcN + 32, rb);
+      QB_TC_LD32(tbase, ra);
+      QB_TC_LD32(tbase + 32, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      float m1 = fminf(min32(ra), min32(rb));
+      float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
+      QB_TC_LD32(tbase + 64, ra);
+      QB_TC_LD32(tbase + 96, rb);
       tc_wait_ld();
       reg_fence32(ra);
       reg_fence32(rb);
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[as]);  // the stage is free once the data is in registers
-      const float m1 = fminf(min32(ra), min32(rb));
-      const float m2 = fminf(fmaf(ghi0, s, min32_shift(ra, Q, s)), fmaf(ghi1, s, min32_shift(rb, Q, s)));
+      if (lane == 0) mbar_arrive(&acc_empty[sp]);
+      m1 = fminf(m1, fminf(min32(ra), min32(rb)));
+      m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
       rmin = fmin3(rmin, m1 + R1, m2 + R2);
       if (--rec_left == 0) {
-        // the two column quarters of a half fold into one record (atomic minima)
         const float wm = warp_min_f(rmin) * P.inv_scale;
         if (lane == 0) {
           float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
@@ -390,7 +401,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
             atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
         }
         ++Jrec;
-        rec_left = 1u << (gl - 1);
+        rec_left = 1u << (gl - 2);
         rmin = inf;
       }
     }

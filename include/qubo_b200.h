@@ -73,11 +73,11 @@ extern "C" {
                                  batch has the same shape (sizes, dtype classes, options); any
                                  other batch is captured anew.  pass1_ms then holds the whole
                                  graph's device time and pass2_ms is 0 */
-#define QB_FLAG_TC_ONE_STATE 8 /* QB_FORM_TC, qb_solve / qb_solve_begin: run the tensor-core
-                                 kernel that reads one state per accumulator instead of the
-                                 default pair form (two states per accumulator: each MMA tile
-                                 also yields the tile that differs in one variable); the answers
-                                 are the same */
+#define QB_FLAG_TC_PAIR 8      /* QB_FORM_TC, qb_solve / qb_solve_begin: run the tensor-core pair
+                                 form, which derives a second state from every accumulator (each
+                                 MMA tile also yields the tile that differs in one variable)
+                                 instead of reading one state per accumulator; the answers are
+                                 the same (qb_autotune may also choose it) */
 #define QB_FLAG_TEST_STALL 2  /* tests only, QB_FORM_TC: the search kernel's tile walk
                                  publishes nothing, so the kernel's bounded waits run out
                                  (about 2 s); the call returns QB_ETIMEOUT and the handle

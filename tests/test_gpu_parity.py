@@ -188,28 +188,29 @@ def test_c_abi_two_phase_matches_single_call(cuda_ok):
 
 @pytest.mark.parametrize("n", [20, 21, 25, 29])
 def test_tensor_core_pair_and_one_state_forms(cuda_ok, n):
-    """Both tensor-core kernels (default: two states per accumulator; QB_FLAG_TC_ONE_STATE:
-    one) against the oracle, integer and float Q, whole problem and three shards."""
+    """Both tensor-core kernels (default: one state per accumulator; QB_FLAG_TC_PAIR: two)
+    against the oracle, integer and float Q, whole problem and three shards."""
     rng = np.random.default_rng(400 + n)
     U = rng.integers(-60, 61, (n, n)).astype(np.int32)
     G = rng.standard_normal((n, n))
     h = _lib.handle(0)
     for Q in (U, (np.triu(U) + np.triu(U, 1).T).astype(np.int32), G, ((G + G.T) / 2).astype(np.float32)):
         ref = oracle.qbf_port(Q)
-        for one in (False, True):
-            r = h.solve(Q, form="tc", tc_one_state=one)
+        for pair in (False, True):
+            r = h.solve(Q, form="tc", tc_pair=pair)
             assert r["form"] == "tc"
             _check(Q, _as_sol(r), ref)
-        mins = []
-        for s in range(3):  # one pending two-phase solve per handle: begin, then finish
-            mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3))
-            h.solve_finish(mins[-1], n)
-        outs = []
-        for s in range(3):
-            h.solve_begin(Q, form="tc", shard_index=s, shard_count=3)
-            outs.append(h.solve_finish(min(mins), n))
-        best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
-        assert best["best_X_int"] == ref["best_X_int"]
+        for pair in (False, True):
+            mins = []
+            for s in range(3):  # one pending two-phase solve per handle: begin, then finish
+                mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3, tc_pair=pair))
+                h.solve_finish(mins[-1], n)
+            outs = []
+            for s in range(3):
+                h.solve_begin(Q, form="tc", shard_index=s, shard_count=3, tc_pair=pair)
+                outs.append(h.solve_finish(min(mins), n))
+            best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
+            assert best["best_X_int"] == ref["best_X_int"]
 
 
 class _as_sol:

@@ -84,14 +84,14 @@ def test_batched_kernel_other_splits(cuda_ok):
 
 
 @pytest.mark.parametrize("n,kind", [(24, "v_row"), (32, "cancel"), (36, "at_limit"), (32, "over_limit")])
-def test_one_state_kernel(cuda_ok, n, kind):
-    """The tensor-core kernel that reads one state per accumulator (QB_FLAG_TC_ONE_STATE) on
-    the same edge cases: the same answer as the default pair form and the oracle."""
+def test_pair_kernel(cuda_ok, n, kind):
+    """The tensor-core pair form (QB_FLAG_TC_PAIR: two states per accumulator) on the same
+    edge cases: the same answer as the default one-state kernel and the oracle."""
     Q = _case(n, kind)
     ref = _ref(n, kind)
     h = _lib.handle(0)
-    one = h.solve(Q, form="tc", tc_one_state=True)
-    two = h.solve(Q, form="tc")
+    one = h.solve(Q, form="tc")
+    two = h.solve(Q, form="tc", tc_pair=True)
     assert (one["best_X_int"], one["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
     assert (two["best_X_int"], two["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
     if kind != "over_limit":
