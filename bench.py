@@ -247,6 +247,7 @@ def bench_ours(args):
     clocks = clk.summary()
     gray_ms, gres = timed("gray", max(3, args.steps // 2), 3)
     pair_ms, pres = timed("tc", max(3, args.steps // 2), 3, tc_pair=True) if form == "tc" else (None, [])
+    f32_ms, fres = timed("tc", max(3, args.steps // 2), 3, tc_no16=True) if form == "tc" else (None, [])
     r0 = res[-1]
     # e2e: the public API with a host-resident problem, H2D and D2H inside the timed region
     prob = Just_Q(Q)
@@ -305,6 +306,9 @@ def bench_ours(args):
         "tc_over_gray": (gray_ms / ms),
         "tc_pair_form": ({"ms_per_step": pair_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in pres)}
                          if pres else None),
+        "tc_fp32_minima": ({"ms_per_step": f32_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in fres)}
+                           if fres else None),
+        "tc_kernel": r0["plan"]["tc_kernel"],
         "clocks": clocks,
     }
     if rank == 0 and world == 1:

@@ -23,6 +23,8 @@ QB_FLAG_INT16_WRAP = 1
 QB_FLAG_TEST_STALL = 2
 QB_FLAG_GRAPH = 4
 QB_FLAG_TC_PAIR = 8
+QB_FLAG_TC_NO16 = 16
+TC_KERNELS = {0: None, 1: "fp32", 2: "pair", 3: "u16"}
 TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
 
 _DTYPES = {
@@ -54,7 +56,7 @@ class QbResult(ctypes.Structure):
                 ("pass1_ms", ctypes.c_float), ("pass2_ms", ctypes.c_float), ("kernels", ctypes.c_int32),
                 ("kernel_ms", ctypes.c_float), ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
                 ("rec_log2", ctypes.c_int32), ("suffix_bits", ctypes.c_int32), ("unit_log2", ctypes.c_int32),
-                ("tuned", ctypes.c_int32)]
+                ("tuned", ctypes.c_int32), ("tc_kernel", ctypes.c_int32)]
 
 
 class QbNoAllocResult(ctypes.Structure):
@@ -153,12 +155,12 @@ class Handle:
     @staticmethod
     def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
                 max_candidates=0, stream=None, int16_wrap=False, flags=0, graph=False,
-                tc_pair=False) -> QbOptions:
+                tc_pair=False, tc_no16=False) -> QbOptions:
         return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
                          prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
                          max_candidates=int(max_candidates),
                          flags=int(flags) | (QB_FLAG_INT16_WRAP if int16_wrap else 0) | (QB_FLAG_GRAPH if graph else 0) |
-                         (QB_FLAG_TC_PAIR if tc_pair else 0),
+                         (QB_FLAG_TC_PAIR if tc_pair else 0) | (QB_FLAG_TC_NO16 if tc_no16 else 0),
                          stream=stream)
 
     def solve(self, Q: np.ndarray, **opts) -> dict:
@@ -329,7 +331,8 @@ def result_row(r, n: int) -> dict:
         "h2d_bytes": int(r["h2d_bytes"]),
         "d2h_bytes": int(r["d2h_bytes"]),
         "plan": {"rec_log2": int(r["rec_log2"]), "suffix_bits": int(r["suffix_bits"]),
-                 "unit_log2": int(r["unit_log2"]), "tuned": bool(r["tuned"])},
+                 "unit_log2": int(r["unit_log2"]), "tuned": bool(r["tuned"]),
+                 "tc_kernel": TC_KERNELS.get(int(r["tc_kernel"]))},
     }
 
 
@@ -355,7 +358,7 @@ def result_dict(r: QbResult, n: int) -> dict:
         "h2d_bytes": int(r.h2d_bytes),
         "d2h_bytes": int(r.d2h_bytes),
         "plan": {"rec_log2": int(r.rec_log2), "suffix_bits": int(r.suffix_bits), "unit_log2": int(r.unit_log2),
-                 "tuned": bool(r.tuned)},
+                 "tuned": bool(r.tuned), "tc_kernel": TC_KERNELS.get(int(r.tc_kernel))},
     }
 
 

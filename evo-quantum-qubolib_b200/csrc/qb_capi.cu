@@ -379,6 +379,7 @@ void fill_plan_fields(const qb_handle* h, const Plan& P, qb_result* r) {
     r->tuned = 0;
   }
   if (T.form && T.form == P.form) r->tuned = 1;
+  r->tc_kernel = P.form != QB_FORM_TC ? 0 : (P.tc.pair ? 2 : (P.tc.u16 ? 3 : 1));
 }
 
 int upload_W(qb_handle* h, const std::vector<double>& W) {
@@ -546,8 +547,10 @@ int begin_launch(qb_handle* h, const qb_problem* p, const qb_options* o, Plan& P
   if (rc) return rc;
   rc = plan_problem(h, o, P);
   if (rc) return rc;
-  if (P.form == QB_FORM_TC)  // pair form: couplings of variable n-16 with the u variables
+  if (P.form == QB_FORM_TC) {  // pair form: couplings of variable n-16 with the u variables
     for (int j = 0; j < 8; ++j) P.tc.gamma[j] = (float)(W[(size_t)(P.n - 16) * P.n + (P.n - 1 - j)] * P.tc.scale);
+    P.tc.u16 = !P.tc.pair && P.tc.exact && !(o->flags & QB_FLAG_TC_NO16) && qb::tc_u16_eligible(P.n, W.data(), &P.tc.dmin);
+  }
   rc = upload_W(h, W);
   if (rc) return rc;
   QB_CUDA(h->misc.ensure(64));

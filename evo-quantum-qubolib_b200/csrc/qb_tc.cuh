@@ -78,7 +78,50 @@ struct TcPlan {
   bool stall = false;      // test hook: the tile walk publishes nothing (waits expire)
   bool pair = false;       // two states per accumulator (tc_pair_kernel, qb_tc2.cuh)
   float gamma[8] = {0};    // pair form: scaled W[n-16][n-1-j], j < 8
+  bool u16 = false;        // 16-bit epilogue (tc_u16_eligible)
+  float dmin = 0.f;        // 16-bit epilogue: lower bound of every accumulator value D
 };
+
+// The 16-bit epilogue.  An accumulator holds D(y, u) = y^T V u + C_t(u), a sum of couplings
+// W_ab with at least one of a, b among the u variables, so Dmin <= D <= Dmax with Dmin (Dmax)
+// the sum of the negative (positive) such couplings.  When Dmax - Dmin < 2^16, every
+// coupling row (V u)_i of a y variable stays within +-2048 (one exact fp16 digit) and integer
+// Q is on the exact path, the MMA computes F = D + 2^23 - Dmin exactly (the column term
+// carries the offset in three fp16 digits: 1, 2048 and 32768 times d0 < 2048, d1 < 16,
+// d2 = 256 or 257): F is an integer in [2^23, 2^24), so the low 16 bits of its fp32 pattern
+// are exactly D - Dmin.  The epilogue then loads the accumulators two per register
+// (tcgen05.ld .pack::16b keeps the low 16 bits of each column) and takes unsigned 16-bit
+// minima (min.u16x2, two states per full-rate ALU instruction, against one 3-input fp32 min
+// per two states at half rate), and holds 128 columns in 64 registers, so each epilogue
+// warp loads its whole half-stage at once and releases it before any arithmetic.
+// W is the n x n FP64 matrix of the problem (unscaled: the exact path has scale 1).
+inline bool tc_u16_eligible(int n, const double* W, float* dmin) {
+  if (n < 20) return false;
+  double lo = 0.0, hi = 0.0;
+  auto add = [&](double w) {
+    if (w < 0) lo += w;
+    else hi += w;
+  };
+  for (int i = 0; i < 7; ++i) {  // y variable n-9-i: its coupling row with the u variables
+    double rp = 0.0, rn = 0.0;
+    for (int j = 0; j < 8; ++j) {
+      const double w = W[(size_t)(n - 9 - i) * n + (n - 1 - j)];
+      if (w < 0) rn -= w;
+      else rp += w;
+      add(w);
+    }
+    if (rp > 2048.0 || rn > 2048.0) return false;
+  }
+  for (int j = 0; j < 8; ++j) {
+    const int a = n - 1 - j;
+    add(W[(size_t)a * n + a]);                                          // u diagonal
+    for (int j2 = 0; j2 < j; ++j2) add(W[(size_t)a * n + (n - 1 - j2)]);  // u-u couplings
+    for (int t = 0; t < n - 15; ++t) add(W[(size_t)t * n + a]);          // t-u couplings
+  }
+  if (hi - lo > 65535.0) return false;
+  *dmin = (float)lo;
+  return true;
+}
 
 // one CTA work item: a contiguous run of whole record blocks of one problem
 struct TcItem {
@@ -104,6 +147,8 @@ struct TcParams {
   const uint32_t* item_first;  //     [item_first[b], item_first[b + 1])
   int n_max;                // largest n among the items (shared-memory layout)
   unsigned* err;            // error word
+  float dmin;               // 16-bit epilogue: lower bound of the accumulator values
+  float k0;                 // 16-bit epilogue: 2^23 - dmin, added to the column term
 };
 
 inline bool tc_supported(int n) { return n >= 20 && n <= kMaxN; }
@@ -207,6 +252,15 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
                : "memory");
 }
 
+// 32 columns as 16 registers, two columns per register (the low 16 bits of each)
+#define QB_TC_LD16P(taddr, r)                                                                                  \
+  asm volatile(                                                                                                \
+      "tcgen05.ld.sync.aligned.32x32b.x16.pack::16b.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, " \
+      "[%16];"                                                                                                 \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),        \
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])   \
+      : "r"(taddr))
+
 #define QB_TC_LD32(taddr, r)                                                                                      \
   asm volatile(                                                                                                   \
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18," \
@@ -226,6 +280,28 @@ __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sy
 __device__ __forceinline__ void reg_fence32(uint32_t* r) {
 #pragma unroll
   for (int i = 0; i < 32; ++i) asm volatile("" : "+r"(r[i]));
+}
+
+__device__ __forceinline__ void reg_fence16(uint32_t* r) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) asm volatile("" : "+r"(r[i]));
+}
+
+__device__ __forceinline__ uint32_t umin2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+  return d;
+}
+
+// unsigned 16-bit minimum over 4 x 16 registers of packed pairs, as an int
+__device__ __forceinline__ uint32_t umin64(uint32_t* a, uint32_t* b, uint32_t* c, uint32_t* d) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) a[i] = umin2(umin2(a[i], b[i]), umin2(c[i], d[i]));
+#pragma unroll
+  for (int w = 8; w >= 1; w >>= 1)
+#pragma unroll
+    for (int i = 0; i < w; ++i) a[i] = umin2(a[i], a[i + w]);
+  return min(a[0] & 0xffffu, a[0] >> 16);
 }
 
 __device__ __forceinline__ float min32(const uint32_t* r) {
@@ -303,8 +379,9 @@ __host__ __device__ inline TcSmemLayout tc_layout(int n) {
 }
 
 // kItems = false: one problem (one work item per CTA, compiled without the item loop's
-// bookkeeping); kItems = true: the CTA's list of work items.
-template <bool kItems>
+// bookkeeping); kItems = true: the CTA's list of work items.  kU16 (one problem only): the
+// 16-bit epilogue (tc_u16_eligible).
+template <bool kItems, bool kU16 = false>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -395,22 +472,40 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
     for (int e = tid; e < 128 * 16; e += kTcThreads) {
       int y = e >> 4, k = e & 15;
       float v;
-      if (k < 14)
+      if (kU16)  // A[y][i] = y_i (i < 7); the column term's digit weights 1, 2048, 32768
+        v = k < 7 ? (float)((y >> k) & 1) : (k == 7 ? 1.0f : (k == 8 ? 2048.0f : (k == 9 ? 32768.0f : 0.0f)));
+      else if (k < 14)
         v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
       else
         v = (k & 1) ? s1 : 1.0f;
       *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
     }
     // B operand, coupling columns (same in every stage)
-    for (int e = tid; e < kTcN * 7; e += kTcThreads) {
-      int u = e / 7, i = e % 7;
-      const double* row = Ws + (n - 9 - i) * n;
-      double v = 0.0;
-      for (int j = 0; j < 8; ++j)
-        if ((u >> j) & 1) v += row[n - 1 - j];
-      __half2 dg = digits((float)v, exact);
-      for (int s = 0; s < kTcBStages; ++s)
-        *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+    if (kU16) {
+      // one exact fp16 value per coupling row (|(V u)_i| <= 2048), zeros in the unused K slots
+      for (int e = tid; e < kTcN * 16; e += kTcThreads) {
+        const int u = e >> 4, k = e & 15;
+        if (k >= 7 && k < 10) continue;  // the column term's digits, written per tile
+        double v = 0.0;
+        if (k < 7) {
+          const double* row = Ws + (n - 9 - k) * n;
+          for (int j = 0; j < 8; ++j)
+            if ((u >> j) & 1) v += row[n - 1 - j];
+        }
+        const __half hv = __float2half_rn((float)v);
+        for (int s = 0; s < kTcBStages; ++s) *reinterpret_cast<__half*>(Bsm + s * kTcN * 32 + kmaj_off(u, k)) = hv;
+      }
+    } else {
+      for (int e = tid; e < kTcN * 7; e += kTcThreads) {
+        int u = e / 7, i = e % 7;
+        const double* row = Ws + (n - 9 - i) * n;
+        double v = 0.0;
+        for (int j = 0; j < 8; ++j)
+          if ((u >> j) & 1) v += row[n - 1 - j];
+        __half2 dg = digits((float)v, exact);
+        for (int s = 0; s < kTcBStages; ++s)
+          *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+      }
     }
     // E_U(u)
     for (int u = tid; u < kTcN; u += kTcThreads) {
@@ -581,6 +676,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         ok = mbar_wait(&p_full[s], (j >> 6) & 1u, abort_flag);
         if (!ok) break;
         __half2 dg[8];
+        __half dl[8];  // 16-bit epilogue: the column term's lowest digit
         float rr[4];
         {
           const TcSlot& sl = slots[s];
@@ -595,7 +691,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
             if (r & 1) cr += f5;
             if (r & 2) cr += f6;
             if (r & 4) cr += f7;
-            dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+            if (kU16) {
+              // C + 2^23 - Dmin, an integer in [2^23, 2^24): digits d0 < 2048, d1 < 16, d2
+              const float c = EU[lane + 32 * r] + cr + P.k0;
+              const float d2 = floorf(c * (1.0f / 32768.0f));
+              const float rem = c - 32768.0f * d2;
+              const float d1 = floorf(rem * (1.0f / 2048.0f));
+              dl[r] = __float2half_rn(rem - 2048.0f * d1);
+              dg[r] = __halves2half2(__float2half_rn(d1), __float2half_rn(d2));
+            } else {
+              dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+            }
           }
           float g5 = sl.et;
 #pragma unroll
@@ -612,8 +718,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         ok = mbar_wait(&b_empty[bs], ((j >> 3) & 1u) ^ 1u, abort_flag);
         if (!ok) break;
         unsigned char* Bst = Bsm + bs * kTcN * 32;
+        if (kU16) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+          for (int r = 0; r < 8; ++r) {
+            *reinterpret_cast<__half*>(Bst + kmaj_off(lane + 32 * r, 7)) = dl[r];
+            *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+        }
 #pragma unroll
         for (int r = 0; r < 4; ++r) Rs[bs * 128 + lane + 32 * r] = rr[r];
         fence_proxy_async();
@@ -654,6 +768,24 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         ok = mbar_wait(&acc_full[sp], (j >> 1) & 1u, abort_flag);
         if (!ok) break;
         tc_fence_after();
+        if (kU16) {
+          // the warp's 128 columns at once, two per register; released before the minima
+          uint32_t r0[16], r1[16], r2[16], r3[16];
+          QB_TC_LD16P(tbase, r0);
+          QB_TC_LD16P(tbase + 32, r1);
+          QB_TC_LD16P(tbase + 64, r2);
+          QB_TC_LD16P(tbase + 96, r3);
+          tc_wait_ld();
+          reg_fence16(r0);
+          reg_fence16(r1);
+          reg_fence16(r2);
+          reg_fence16(r3);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[sp]);
+          // min over the row of D - Dmin, then E = that + Dmin + R (all exact integers in fp32)
+          rmin = fminf(rmin, (float)umin64(r0, r1, r2, r3) + (R + P.dmin));
+        } else {
         uint32_t ra[32], rb[32];
         QB_TC_LD32(tbase, ra);
         QB_TC_LD32(tbase + 32, rb);
@@ -671,6 +803,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
         if (lane == 0) mbar_arrive(&acc_empty[sp]);  // the stage is free once the data is in registers
         const float m = fminf(m1, fminf(min32(ra), min32(rb)));
         rmin = fminf(rmin, m + R);
+        }
         if (--rec_left == 0) {
           // both parities' warps of (column half, lane quarter) fold into one record
           // the multi-item kernel re-reads the item's record base and scale from shared memory
@@ -747,13 +880,14 @@ inline int tc_launch(const TcPlan& p, float* rec, void* scratch, cudaStream_t st
   P.rec = rec;
   P.err = err;
   P.stall = p.stall ? 1 : 0;
+  P.dmin = p.dmin;
+  P.k0 = 8388608.0f - p.dmin;
   const TcSmemLayout L = tc_layout(p.n);
   // at least 120 KB so that one CTA (and one 512-column TMEM allocation) runs per SM
   const size_t smem = std::max<size_t>(L.total, 120 * 1024) + 1024;
-  if (cudaFuncSetAttribute(tc_pass1_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-      cudaSuccess)
-    return 4;
-  tc_pass1_kernel<false><<<(unsigned)ctas, kTcThreads, smem, st>>>(P);
+  auto kern = p.u16 ? tc_pass1_kernel<false, true> : tc_pass1_kernel<false, false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 4;
+  kern<<<(unsigned)ctas, kTcThreads, smem, st>>>(P);
   ++*kernels;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

@@ -220,3 +220,48 @@ class _as_sol:
         self.best_X = r["best_X"]
         self.best_E = r["best_E"]
         self.search = r
+
+
+@pytest.mark.parametrize("n,hi,seed", [(20, 100, 1), (24, 100, 2), (29, 60, 3), (33, 40, 4), (36, 25, 5)])
+def test_tensor_core_16bit_epilogue(cuda_ok, n, hi, seed):
+    """Integer Q whose accumulator values span fewer than 2^16 integers runs the 16-bit
+    epilogue (exact unsigned 16-bit minima over packed TMEM loads): the oracle's answer, the
+    exact minimum as pass-1 minimum, and the same result as the fp32 minima (QB_FLAG_TC_NO16),
+    whole problem and three shards."""
+    rng = np.random.default_rng(900 + seed)
+    Q = rng.integers(-hi, hi + 1, (n, n)).astype(np.int32)
+    ref = oracle.qbf_port(Q)
+    h = _lib.handle(0)
+    r16 = h.solve(Q, form="tc")
+    r32 = h.solve(Q, form="tc", tc_no16=True)
+    assert r16["plan"]["tc_kernel"] == "u16" and r32["plan"]["tc_kernel"] == "fp32"
+    for r in (r16, r32):
+        assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
+        assert r["pass1_min"] == ref["best_E"] or (ref["best_E"] == 0 and r["pass1_min"] >= 0)
+    mins = []
+    for s in range(3):
+        mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3))
+        h.solve_finish(mins[-1], n)
+    outs = []
+    for s in range(3):
+        h.solve_begin(Q, form="tc", shard_index=s, shard_count=3)
+        outs.append(h.solve_finish(min(mins), n))
+    best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
+    assert best["best_X_int"] == ref["best_X_int"]
+
+
+def test_tensor_core_16bit_epilogue_applies_only_in_range(cuda_ok):
+    """A coupling row beyond +-2048 or a value span of 2^16 or more keeps the fp32 minima."""
+    rng = np.random.default_rng(77)
+    n = 26
+    h = _lib.handle(0)
+    wide = rng.integers(-100, 101, (n, n)).astype(np.int32)
+    wide[n - 9, n - 8:] = 400  # one coupling row of a y variable sums to 3200
+    span = rng.integers(-2000, 2001, (n, n)).astype(np.int32)
+    for Q in (wide, span):
+        r = h.solve(Q, form="tc")
+        assert r["plan"]["tc_kernel"] == "fp32"
+        ref = oracle.qbf_port(Q)
+        assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
+    f = h.solve(rng.standard_normal((n, n)), form="tc")
+    assert f["plan"]["tc_kernel"] == "fp32"
