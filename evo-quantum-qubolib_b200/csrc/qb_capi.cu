@@ -1467,6 +1467,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     } else if (I.kind == qb::kBatchTC) {
       R.rec_log2 = I.gl;
       R.suffix_bits = 15;
+      R.tc_kernel = 1;  // the batch's tensor-core items take fp32 minima
       R.tuned = (T.tc_gl || T.form == QB_FORM_TC) ? 1 : 0;
     } else {
       R.rec_log2 = I.fbits;
