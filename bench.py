@@ -4,6 +4,9 @@ restatement of the reference timed beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--form tc|gray]
 
+The tensor-core form runs its default kernel (for this problem the 16-bit pair form: one MMA
+accumulator per two states); the other tensor-core kernels are timed beside it.
+
 One step = one full exhaustive solve (pass 1 over all 2^36 states, candidate re-evaluation,
 tie rule) of the same problem.  For N > 1 (torchrun, one process per GPU) every rank searches
 its share of the tiles and the ranks exchange their minima (NCCL); the job is the same
@@ -24,8 +27,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 # algorithmic work per state of the contraction: one K = 16 dot product (7 coupling bits x 2
-# digits + 2 column-term digits) = 16 multiply-adds, one MMA accumulator element per state
+# digits + 2 column-term digits) = 16 multiply-adds, one MMA accumulator element per state.
+# The pair kernels execute half of it on the tensor pipe (one accumulator per two states).
 FLOPS_PER_STATE_TC = 32
+TC_VARIANTS = {"u16": {"tc_one": True}, "fp32": {"tc_no16": True}, "pair": {"tc_pair": True, "tc_no16": True}}
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
 
@@ -240,14 +245,20 @@ def bench_ours(args):
         return float(t.item()) / steps, res
 
     form = args.form
-    if form == "tc_pair":
-        raise SystemExit("--form tc_pair is a profiling case option (--case cfg2 or n36); the headline times it beside tc")
+    if form in ("tc_pair", "tc_one"):
+        raise SystemExit(f"--form {form} is a profiling case option (--case cfg2 or n36); the headline times it beside tc")
     with ClockSampler(local) as clk:
         ms, res = timed(form, args.steps, args.warmup)
     clocks = clk.summary()
     gray_ms, gres = timed("gray", max(3, args.steps // 2), 3)
-    pair_ms, pres = timed("tc", max(3, args.steps // 2), 3, tc_pair=True) if form == "tc" else (None, [])
-    f32_ms, fres = timed("tc", max(3, args.steps // 2), 3, tc_no16=True) if form == "tc" else (None, [])
+    variants = {}
+    if form == "tc":  # the other tensor-core kernels on the same problem
+        for name, kw in TC_VARIANTS.items():
+            if name == res[-1]["plan"]["tc_kernel"]:
+                continue
+            v_ms, vres = timed("tc", max(3, args.steps // 2), 3, **kw)
+            variants[name] = {"ms_per_step": v_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in vres),
+                              "tc_kernel": vres[-1]["plan"]["tc_kernel"]}
     r0 = res[-1]
     # e2e: the public API with a host-resident problem, H2D and D2H inside the timed region
     prob = Just_Q(Q)
@@ -277,7 +288,9 @@ def bench_ours(args):
     peak, peak_sus, peak_kind = _peaks()
     local_states = r0["states"] if world == 1 else r0["states"]
     achieved = local_states * FLOPS_PER_STATE_TC / (kernel_ms * 1e-3) / 1e12
-    kernel_name = "tc_pass1_kernel" if form == "tc" else "gray_pass1_kernel"
+    tck = r0["plan"]["tc_kernel"] or ""
+    kernel_name = ("tc_pair_kernel" if tck.startswith("pair") else "tc_pass1_kernel") if form == "tc" else "gray_pass1_kernel"
+    tensor_flops = FLOPS_PER_STATE_TC // 2 if tck.startswith("pair") else FLOPS_PER_STATE_TC
     line = {
         "metric": "states/s (exhaustive QUBO, exact argmin)",
         "value": states / (ms * 1e-3),
@@ -300,15 +313,13 @@ def bench_ours(args):
                      "frac": achieved / peak, "traffic": _traffic(kernel_name, local_states),
                      "kernel": kernel_name,
                      "peak_kind": f"bf16 dense burst, {peak_kind}", "kernel_ms": kernel_ms,
-                     "flops_per_state": FLOPS_PER_STATE_TC},
+                     "flops_per_state": FLOPS_PER_STATE_TC, "tensor_flops_per_state": tensor_flops,
+                     "frac_tensor_pipe": achieved * tensor_flops / FLOPS_PER_STATE_TC / peak},
         "gray_form": {"value": states / (gray_ms * 1e-3), "ms_per_step": gray_ms,
                       "kernel_ms": statistics.mean(r["kernel_ms"] for r in gres)},
         "tc_over_gray": (gray_ms / ms),
-        "tc_pair_form": ({"ms_per_step": pair_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in pres)}
-                         if pres else None),
-        "tc_fp32_minima": ({"ms_per_step": f32_ms, "kernel_ms": statistics.mean(r["kernel_ms"] for r in fres)}
-                           if fres else None),
         "tc_kernel": r0["plan"]["tc_kernel"],
+        "tc_variants": variants or None,
         "clocks": clocks,
     }
     if rank == 0 and world == 1:
@@ -326,7 +337,8 @@ def bench_case(args):
     """Profiling cases, solved `steps` times with one form, one line per solve: cfg2 = the
     32-variable integer QUBO (RandomQUBO seed 0, entries in [-100, 100], symmetric int16);
     n36 = the headline 36-variable TSP QUBO.  Used for ncu captures of a single kernel (a few
-    MB on the device).  --form tc_pair runs the tensor-core pair form."""
+    MB on the device).  --form tc runs the tensor-core form's default kernel, tc_pair the pair
+    form, tc_one one state per accumulator."""
     import torch
     import qubo_b200  # noqa: F401
     from qubo_b200 import _lib, configs
@@ -335,12 +347,13 @@ def bench_case(args):
     name = "random_i16_n32" if args.case == "cfg2" else "tsp6_int_n36"
     h = _lib.handle(0)
     stream = torch.cuda.current_stream(0).cuda_stream
-    form, kw = (("tc", {"tc_pair": True}) if args.form == "tc_pair" else (args.form, {}))
+    form, kw = {"tc_pair": ("tc", {"tc_pair": True}), "tc_one": ("tc", {"tc_one": True})}.get(args.form, (args.form, {}))
     for k in range(args.warmup + args.steps):
         r = h.solve(Q, form=form, stream=stream, **kw)
         if k >= args.warmup:
             print(json.dumps({"case": name, "form": args.form, "best_E": r["best_E"], "states": r["states"],
-                              "kernel_ms": r["kernel_ms"], "pass1_ms": r["pass1_ms"], "pass2_ms": r["pass2_ms"]}),
+                              "kernel_ms": r["kernel_ms"], "pass1_ms": r["pass1_ms"], "pass2_ms": r["pass2_ms"],
+                              "tc_kernel": r["plan"]["tc_kernel"]}),
                   flush=True)
 
 
@@ -440,7 +453,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto", "tc_pair"])
+    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto", "tc_pair", "tc_one"])
     ap.add_argument("--case", default=None, choices=["cfg2", "n36", "batch"],
                     help="cfg2, n36: profiling cases (one line per solve); batch: the 4096-instance batch line")
     args = ap.parse_args()

@@ -24,7 +24,8 @@ QB_FLAG_TEST_STALL = 2
 QB_FLAG_GRAPH = 4
 QB_FLAG_TC_PAIR = 8
 QB_FLAG_TC_NO16 = 16
-TC_KERNELS = {0: None, 1: "fp32", 2: "pair", 3: "u16"}
+QB_FLAG_TC_ONE = 32
+TC_KERNELS = {0: None, 1: "fp32", 2: "pair", 3: "u16", 4: "pair_u16"}
 TIE_RULES = {"qbf": 0, "qb_f1": 1, "natural": 2}
 
 _DTYPES = {
@@ -155,12 +156,13 @@ class Handle:
     @staticmethod
     def options(form="auto", tie_rule="qbf", fixed_bits=0, prefix_bits=-1, shard_index=0, shard_count=1,
                 max_candidates=0, stream=None, int16_wrap=False, flags=0, graph=False,
-                tc_pair=False, tc_no16=False) -> QbOptions:
+                tc_pair=False, tc_no16=False, tc_one=False) -> QbOptions:
         return QbOptions(form=FORMS[form], tie_rule=TIE_RULES[tie_rule], fixed_bits=int(fixed_bits),
                          prefix_bits=int(prefix_bits), shard_index=int(shard_index), shard_count=int(shard_count),
                          max_candidates=int(max_candidates),
                          flags=int(flags) | (QB_FLAG_INT16_WRAP if int16_wrap else 0) | (QB_FLAG_GRAPH if graph else 0) |
-                         (QB_FLAG_TC_PAIR if tc_pair else 0) | (QB_FLAG_TC_NO16 if tc_no16 else 0),
+                         (QB_FLAG_TC_PAIR if tc_pair else 0) | (QB_FLAG_TC_NO16 if tc_no16 else 0) |
+                         (QB_FLAG_TC_ONE if tc_one else 0),
                          stream=stream)
 
     def solve(self, Q: np.ndarray, **opts) -> dict:

@@ -348,7 +348,8 @@ int plan_problem(qb_handle* h, const qb_options* o, Plan& P) {
   // tensor-core form
   qb::tc_plan(n, P.is_int, P.abs_sum, shard_idx, shard_cnt, &P.tc, T.tc_gl);
   P.tc.stall = (o->flags & QB_FLAG_TEST_STALL) != 0;
-  P.tc.pair = (o->flags & QB_FLAG_TC_PAIR) != 0 || T.tc_pair;
+  if ((o->flags & QB_FLAG_TC_PAIR) && (o->flags & QB_FLAG_TC_ONE)) return QB_EINVAL;
+  P.tc.pair = (o->flags & QB_FLAG_TC_PAIR) != 0 || (!(o->flags & QB_FLAG_TC_ONE) && T.tc_pair);
   if (P.tc.pair && !P.tc.exact) P.tc.eps = qb::tc2_error_bound(P.abs_sum);
   P.geom.kind = qb::kGeomTC;
   P.geom.gl = P.tc.gl;
@@ -379,7 +380,7 @@ void fill_plan_fields(const qb_handle* h, const Plan& P, qb_result* r) {
     r->tuned = 0;
   }
   if (T.form && T.form == P.form) r->tuned = 1;
-  r->tc_kernel = P.form != QB_FORM_TC ? 0 : (P.tc.pair ? 2 : (P.tc.u16 ? 3 : 1));
+  r->tc_kernel = P.form != QB_FORM_TC ? 0 : (P.tc.pair ? (P.tc.u16 ? 4 : 2) : (P.tc.u16 ? 3 : 1));
 }
 
 int upload_W(qb_handle* h, const std::vector<double>& W) {
@@ -549,7 +550,14 @@ int begin_launch(qb_handle* h, const qb_problem* p, const qb_options* o, Plan& P
   if (rc) return rc;
   if (P.form == QB_FORM_TC) {  // pair form: couplings of variable n-16 with the u variables
     for (int j = 0; j < 8; ++j) P.tc.gamma[j] = (float)(W[(size_t)(P.n - 16) * P.n + (P.n - 1 - j)] * P.tc.scale);
-    P.tc.u16 = !P.tc.pair && P.tc.exact && !(o->flags & QB_FLAG_TC_NO16) && qb::tc_u16_eligible(P.n, W.data(), &P.tc.dmin);
+    const bool no16 = (o->flags & QB_FLAG_TC_NO16) != 0;
+    // default kernel where neither a flag nor the tuned entry names one: the 16-bit pair form
+    // wherever it applies (the fastest measured), else one state per accumulator
+    const qb_handle::Tuned& T = h->tuned[P.is_int ? 1 : 0][P.n];
+    if (!P.tc.pair && P.tc.exact && !no16 && !(o->flags & QB_FLAG_TC_ONE) && T.form != QB_FORM_TC)
+      P.tc.pair = qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin);
+    P.tc.u16 = P.tc.exact && !no16 &&
+               (P.tc.pair ? qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin) : qb::tc_u16_eligible(P.n, W.data(), &P.tc.dmin));
   }
   rc = upload_W(h, W);
   if (rc) return rc;

@@ -95,7 +95,8 @@ struct TcPlan {
 // per two states at half rate), and holds 128 columns in 64 registers, so each epilogue
 // warp loads its whole half-stage at once and releases it before any arithmetic.
 // W is the n x n FP64 matrix of the problem (unscaled: the exact path has scale 1).
-inline bool tc_u16_eligible(int n, const double* W, float* dmin) {
+// span (optional) receives Dmax - Dmin.
+inline bool tc_u16_eligible(int n, const double* W, float* dmin, double* span = nullptr) {
   if (n < 20) return false;
   double lo = 0.0, hi = 0.0;
   auto add = [&](double w) {
@@ -120,6 +121,7 @@ inline bool tc_u16_eligible(int n, const double* W, float* dmin) {
   }
   if (hi - lo > 65535.0) return false;
   *dmin = (float)lo;
+  if (span) *span = hi - lo;
   return true;
 }
 

@@ -21,12 +21,34 @@
 // both tiles.  Records: per block of 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in
 // qb_tc.cuh (kGeomTC); a pair never straddles two blocks.
 //
+// The 16-bit pair form (kU16, tc2_u16_eligible).  As in the one-state 16-bit epilogue
+// (qb_tc.cuh, tc_u16_eligible), the MMA computes F = D + 2^23 - Dmin, whose fp32 pattern
+// holds D - Dmin in its low 16 bits, and the epilogue loads the accumulators two columns per
+// register (.pack::16b, column 2k in the low half of register k of a 32-column chunk).  The
+// partner tile's accumulator D' = D + s * gamma(u) lies in [Dmin, Dmax] as well, so its
+// 16-bit value is (D - Dmin) + s * gamma(u) taken mod 2^16 with no loss.  Per register of a
+// chunk one add.u16x2 of K_s[k] = s * g5(col) + B_s (col = 2k, 2k + 1; the same 16 constants
+// in every chunk, so they stay in registers) and packed 3-input minima give the chunk's
+// partner minimum shifted by B_s - s * ghi(chunk), ghi the gamma of u bits 5..7;
+// B_s = max over the 8 chunks of s * ghi keeps every shifted value in [0, 2^16) when
+// Dmax - Dmin + sum_{b=5..7} |gamma_b| < 2^16, and one add.u16x2 per chunk takes the shift
+// off.  Measured on B200: packed 16-bit minima (2- or 3-input) issue at half rate on the ALU
+// pipe, add.u16x2 at half rate on the FMA pipe, so the partner's adds run beside the
+// minima; per register of 4 states the epilogue spends 2 ALU and 2 FMA issue cycles.  Each
+// warp's pairs share one parity, hence one sign s: one of two copies of the loop.  Constants
+// that differ per chunk (64 per warp) did not stay in registers and ran 25 % slower.
+//
 // Exactness: for integer Q with sum|Q| <= 2^22, D + s*gamma(u) = y^T V u + C_t'(u) is an
 // integer of magnitude at most sum|Q| (it is the accumulator tile t' would have had), so the
 // fma is exact.  For float Q, gamma in fp32, its partial sums g5, the fma and the chunk
 // offset add at most 8 roundings of 2^-24 relative to sum|Q| (scaled units) to the error
 // bound of the digit contraction; tc2_error_bound() includes them.
 #pragma once
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <type_traits>
+
 #include "qb_tc.cuh"
 
 namespace qb {
@@ -38,7 +60,51 @@ struct Tc2Params {
   TcParams P;       // n, nt, gl, stall, exact, inv_scale, W, tile_begin, groups, groups_per_cta, rec, err
   alignas(8) float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
   float whi[3];     // w_5, w_6, w_7: gamma of u bits 5..7 (scaled W)
+  uint32_t k16[2][16];    // 16-bit form: K_s of register k, [0] for s = +1, [1] for s = -1
+  uint32_t corr16[2][8];  // 16-bit form: s * ghi(c) - B_s mod 2^16 in both halves, chunk c = u >> 5
 };
+
+// The 16-bit pair form applies (integer Q on the exact path; W unscaled, n x n FP64): the
+// problems of the one-state 16-bit epilogue with room for the chunk shifts,
+// Dmax - Dmin + sum_{b=5..7} |gamma_b| < 2^16.
+inline bool tc2_u16_eligible(int n, const double* W, float* dmin) {
+  double span = 0.0;
+  if (!tc_u16_eligible(n, W, dmin, &span)) return false;
+  double ghi = 0.0;
+  for (int b = 5; b < 8; ++b) ghi += std::fabs(W[(size_t)(n - 16) * n + (n - 1 - b)]);
+  return span + ghi <= 65535.0;
+}
+
+// the 16-bit pair form's constant tables from gamma (integers on the exact path)
+inline void tc2_u16_tables(const float* gamma, Tc2Params* Q) {
+  int64_t g[8];
+  for (int j = 0; j < 8; ++j) g[j] = (int64_t)std::llrint(gamma[j]);
+  for (int neg = 0; neg < 2; ++neg) {
+    const int64_t s = neg ? -1 : 1;
+    int64_t ghi[8], B = INT64_MIN;
+    for (int c = 0; c < 8; ++c) {
+      ghi[c] = 0;
+      for (int b = 0; b < 3; ++b)
+        if ((c >> b) & 1) ghi[c] += g[5 + b];
+      B = std::max(B, s * ghi[c]);
+    }
+    for (int k = 0; k < 16; ++k) {
+      uint32_t h[2];
+      for (int d = 0; d < 2; ++d) {
+        const int col = 2 * k + d;
+        int64_t g5 = 0;
+        for (int b = 0; b < 5; ++b)
+          if ((col >> b) & 1) g5 += g[b];
+        h[d] = (uint32_t)((s * g5 + B) & 0xffff);
+      }
+      Q->k16[neg][k] = h[0] | (h[1] << 16);
+    }
+    for (int c = 0; c < 8; ++c) {
+      const uint32_t v = (uint32_t)((s * ghi[c] - B) & 0xffff);
+      Q->corr16[neg][c] = v | (v << 16);
+    }
+  }
+}
 
 #ifdef __CUDACC__
 
@@ -74,6 +140,31 @@ __device__ __forceinline__ float min32_shift(const uint32_t* r, const Tc2Params&
   return fmin3(n0, n1, fminf(n2, n3));
 }
 
+__device__ __forceinline__ uint32_t uadd2(uint32_t a, uint32_t b) {
+  uint32_t d;
+  asm("add.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));  // per half, mod 2^16
+  return d;
+}
+
+// packed unsigned 16-bit minima over the 16 registers of a 32-column chunk (3-input minima)
+__device__ __forceinline__ uint32_t umin16(const uint32_t* r) {
+  const uint32_t a = __vimin3_u16x2(r[0], r[1], r[2]), b = __vimin3_u16x2(r[3], r[4], r[5]);
+  const uint32_t c = __vimin3_u16x2(r[6], r[7], r[8]), d = __vimin3_u16x2(r[9], r[10], r[11]);
+  const uint32_t e = __vimin3_u16x2(r[12], r[13], r[14]);
+  return __vimin3_u16x2(__vimin3_u16x2(a, b, c), __vimin3_u16x2(d, e, r[15]), 0xffffffffu);
+}
+
+// the partner tile's packed minima of one chunk, shifted by B_s - s * ghi(chunk): r + K_s per
+// register (16 constants of the sign, the same in every chunk), then packed minima
+template <int kNeg>
+__device__ __forceinline__ uint32_t umin16_shift(const uint32_t* r, const Tc2Params& Q) {
+  uint32_t v[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = uadd2(r[k], Q.k16[kNeg][k]);
+  return umin16(v);
+}
+
+template <bool kU16>
 __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_constant__ Tc2Params Q) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   const TcParams& P = Q.P;
@@ -130,24 +221,44 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
   for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
   for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
   __syncthreads();
+  // A operand (constant); the 16-bit form as in tc_pass1_kernel<false, true>
   for (int e = tid; e < 128 * 16; e += kTcThreads) {
     int y = e >> 4, k = e & 15;
     float v;
-    if (k < 14)
+    if (kU16)  // A[y][i] = y_i (i < 7); the column term's digit weights 1, 2048, 32768
+      v = k < 7 ? (float)((y >> k) & 1) : (k == 7 ? 1.0f : (k == 8 ? 2048.0f : (k == 9 ? 32768.0f : 0.0f)));
+    else if (k < 14)
       v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
     else
       v = (k & 1) ? s1 : 1.0f;
     *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
   }
-  for (int e = tid; e < kTcN * 7; e += kTcThreads) {
-    int u = e / 7, i = e % 7;
-    const double* row = Ws + (n - 9 - i) * n;
-    double v = 0.0;
-    for (int j = 0; j < 8; ++j)
-      if ((u >> j) & 1) v += row[n - 1 - j];
-    __half2 dg = digits((float)v, exact);
-    for (int s = 0; s < kTcBStages; ++s)
-      *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+  // B operand, coupling columns (same in every stage)
+  if (kU16) {
+    // one exact fp16 value per coupling row (|(V u)_i| <= 2048), zeros in the unused K slots
+    for (int e = tid; e < kTcN * 16; e += kTcThreads) {
+      const int u = e >> 4, k = e & 15;
+      if (k >= 7 && k < 10) continue;  // the column term's digits, written per pair
+      double v = 0.0;
+      if (k < 7) {
+        const double* row = Ws + (n - 9 - k) * n;
+        for (int j = 0; j < 8; ++j)
+          if ((u >> j) & 1) v += row[n - 1 - j];
+      }
+      const __half hv = __float2half_rn((float)v);
+      for (int s = 0; s < kTcBStages; ++s) *reinterpret_cast<__half*>(Bsm + s * kTcN * 32 + kmaj_off(u, k)) = hv;
+    }
+  } else {
+    for (int e = tid; e < kTcN * 7; e += kTcThreads) {
+      int u = e / 7, i = e % 7;
+      const double* row = Ws + (n - 9 - i) * n;
+      double v = 0.0;
+      for (int j = 0; j < 8; ++j)
+        if ((u >> j) & 1) v += row[n - 1 - j];
+      __half2 dg = digits((float)v, exact);
+      for (int s = 0; s < kTcBStages; ++s)
+        *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
+    }
   }
   for (int u = tid; u < kTcN; u += kTcThreads) {
     double e = 0.0;
@@ -294,6 +405,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       ok = mbar_wait(&p_full[sa], (ja >> 6) & 1u, abort_flag) && mbar_wait(&p_full[sb], (jb >> 6) & 1u, abort_flag);
       if (!ok) break;
       __half2 dg[8];
+      __half dl[8];  // 16-bit form: the column term's lowest digit
       float ra[4], rb[4];
       {
         const TcSlot& sl = slots[sa];
@@ -308,7 +420,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
           if (r & 1) cr += f5;
           if (r & 2) cr += f6;
           if (r & 4) cr += f7;
-          dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+          if (kU16) {
+            // C + 2^23 - Dmin, an integer in [2^23, 2^24): digits d0 < 2048, d1 < 16, d2
+            const float c = EU[lane + 32 * r] + cr + P.k0;
+            const float d2 = floorf(c * (1.0f / 32768.0f));
+            const float rem = c - 32768.0f * d2;
+            const float d1 = floorf(rem * (1.0f / 2048.0f));
+            dl[r] = __float2half_rn(rem - 2048.0f * d1);
+            dg[r] = __halves2half2(__float2half_rn(d1), __float2half_rn(d2));
+          } else {
+            dg[r] = digits(EU[lane + 32 * r] + cr, exact);
+          }
         }
       }
 #pragma unroll
@@ -329,8 +451,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       ok = mbar_wait(&b_empty[bs], ((p >> 3) & 1u) ^ 1u, abort_flag);
       if (!ok) break;
       unsigned char* Bst = Bsm + bs * kTcN * 32;
+      if (kU16) {
 #pragma unroll
-      for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+        for (int r = 0; r < 8; ++r) {
+          *reinterpret_cast<__half*>(Bst + kmaj_off(lane + 32 * r, 7)) = dl[r];
+          *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
+      }
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         Rs[bs * 128 + lane + 32 * r] = ra[r];
@@ -351,58 +481,119 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
     const int y = q * 32 + lane;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
-    const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
-    const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
-    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
-    // gamma of u bits 5..7 for the four 32-column chunks of this half
-    float ghi[4];
+    if (kU16) {
+      const uint32_t sp = (uint32_t)cq >> 1;  // pair parity = accumulator stage
+      const uint32_t hh = (uint32_t)cq & 1u;  // column half: u bit 7
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+      // every pair of this warp has parity sp, so one sign: s = -1 when tile 2p has t bit 0 set
+      const uint32_t neg = (uint32_t)(((i_begin >> 1) + sp) & 1ull);
+      uint32_t corr[4];  // chunk shifts of this half (u bits 5, 6 = chunk, bit 7 = hh)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
-    // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
-    uint32_t rec_left = 1u << (gl - 2);
-    uint32_t Jrec = 0;
-    for (uint32_t p = sp; p < npairs && ok; p += 2) {
-      const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-      ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
-      if (!ok) break;
-      const float R1 = Rs[bs * 128 + y];
-      const float R2 = Rs2[bs * 128 + y];
-      // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
-      const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
-      ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
-      if (!ok) break;
-      tc_fence_after();
-      uint32_t ra[32], rb[32];
-      QB_TC_LD32(tbase, ra);
-      QB_TC_LD32(tbase + 32, rb);
-      tc_wait_ld();
-      reg_fence32(ra);
-      reg_fence32(rb);
-      float m1 = fminf(min32(ra), min32(rb));
-      float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
-      QB_TC_LD32(tbase + 64, ra);
-      QB_TC_LD32(tbase + 96, rb);
-      tc_wait_ld();
-      reg_fence32(ra);
-      reg_fence32(rb);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[sp]);
-      m1 = fminf(m1, fminf(min32(ra), min32(rb)));
-      m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
-      rmin = fmin3(rmin, m1 + R1, m2 + R2);
-      if (--rec_left == 0) {
-        const float wm = warp_min_f(rmin) * P.inv_scale;
-        if (lane == 0) {
-          float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
-          if (wm >= 0.f)
-            atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
-          else
-            atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+      for (int c = 0; c < 4; ++c) corr[c] = Q.corr16[neg][(hh << 2) | (uint32_t)c];
+      auto pairs = [&](auto kneg) {
+        constexpr int kN = decltype(kneg)::value;
+        uint32_t rec_left = 1u << (gl - 2);
+        uint32_t Jrec = 0;
+        for (uint32_t p = sp; p < npairs && ok; p += 2) {
+          const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+          ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
+          if (!ok) break;
+          const float R1 = Rs[bs * 128 + y] + P.dmin;
+          const float R2 = Rs2[bs * 128 + y] + P.dmin;
+          ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
+          if (!ok) break;
+          tc_fence_after();
+          // the warp's 128 columns at once, two per register; released before the minima
+          uint32_t r[4][16];
+          QB_TC_LD16P(tbase, r[0]);
+          QB_TC_LD16P(tbase + 32, r[1]);
+          QB_TC_LD16P(tbase + 64, r[2]);
+          QB_TC_LD16P(tbase + 96, r[3]);
+          tc_wait_ld();
+#pragma unroll
+          for (int c = 0; c < 4; ++c) reg_fence16(r[c]);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&acc_empty[sp]);
+          // tile 2p: packed minima of D - Dmin; tile 2p + 1: packed minima of the shifted
+          // partner values, unshifted per chunk (mod 2^16, exact: every true value is in range)
+          const uint32_t m1 = umin2(umin2(umin16(r[0]), umin16(r[1])), umin2(umin16(r[2]), umin16(r[3])));
+          const uint32_t m2 = umin2(umin2(uadd2(umin16_shift<kN>(r[0], Q), corr[0]), uadd2(umin16_shift<kN>(r[1], Q), corr[1])),
+                                    umin2(uadd2(umin16_shift<kN>(r[2], Q), corr[2]), uadd2(umin16_shift<kN>(r[3], Q), corr[3])));
+          rmin = fmin3(rmin, (float)min(m1 & 0xffffu, m1 >> 16) + R1, (float)min(m2 & 0xffffu, m2 >> 16) + R2);
+          if (--rec_left == 0) {
+            const float wm = warp_min_f(rmin) * P.inv_scale;
+            if (lane == 0) {
+              float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+              if (wm >= 0.f)
+                atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+              else
+                atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+            }
+            ++Jrec;
+            rec_left = 1u << (gl - 2);
+            rmin = inf;
+          }
         }
-        ++Jrec;
-        rec_left = 1u << (gl - 2);
-        rmin = inf;
+      };
+      if (neg)
+        pairs(std::integral_constant<int, 1>());
+      else
+        pairs(std::integral_constant<int, 0>());
+    } else {
+      const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
+      const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+      // gamma of u bits 5..7 for the four 32-column chunks of this half
+      float ghi[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
+      // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
+      uint32_t rec_left = 1u << (gl - 2);
+      uint32_t Jrec = 0;
+      for (uint32_t p = sp; p < npairs && ok; p += 2) {
+        const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+        ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
+        if (!ok) break;
+        const float R1 = Rs[bs * 128 + y];
+        const float R2 = Rs2[bs * 128 + y];
+        // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
+        const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
+        ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
+        if (!ok) break;
+        tc_fence_after();
+        uint32_t ra[32], rb[32];
+        QB_TC_LD32(tbase, ra);
+        QB_TC_LD32(tbase + 32, rb);
+        tc_wait_ld();
+        reg_fence32(ra);
+        reg_fence32(rb);
+        float m1 = fminf(min32(ra), min32(rb));
+        float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
+        QB_TC_LD32(tbase + 64, ra);
+        QB_TC_LD32(tbase + 96, rb);
+        tc_wait_ld();
+        reg_fence32(ra);
+        reg_fence32(rb);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[sp]);
+        m1 = fminf(m1, fminf(min32(ra), min32(rb)));
+        m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
+        rmin = fmin3(rmin, m1 + R1, m2 + R2);
+        if (--rec_left == 0) {
+          const float wm = warp_min_f(rmin) * P.inv_scale;
+          if (lane == 0) {
+            float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+            if (wm >= 0.f)
+              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+            else
+              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+          }
+          ++Jrec;
+          rec_left = 1u << (gl - 2);
+          rmin = inf;
+        }
       }
     }
   }
@@ -453,11 +644,16 @@ inline int tc2_launch(const TcPlan& p, const float* gamma, float* rec, void* scr
   Q.whi[0] = gamma[5];
   Q.whi[1] = gamma[6];
   Q.whi[2] = gamma[7];
+  if (p.u16) {
+    P.dmin = p.dmin;
+    P.k0 = 8388608.0f - p.dmin;
+    tc2_u16_tables(gamma, &Q);
+  }
   const TcSmemLayout L = tc_layout(p.n);
   const size_t smem = std::max<size_t>(L.total + kTcBStages * 128 * 4, 120 * 1024) + 1024;
-  if (cudaFuncSetAttribute(tc_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return 4;
-  tc_pair_kernel<<<(unsigned)ctas, kTcThreads, smem, st>>>(Q);
+  auto* kern = p.u16 ? tc_pair_kernel<true> : tc_pair_kernel<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 4;
+  kern<<<(unsigned)ctas, kTcThreads, smem, st>>>(Q);
   ++*kernels;
   return cudaGetLastError() == cudaSuccess ? 0 : 4;
 }

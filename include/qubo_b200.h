@@ -78,8 +78,14 @@ extern "C" {
                                  MMA tile also yields the tile that differs in one variable)
                                  instead of reading one state per accumulator; the answers are
                                  the same (qb_autotune may also choose it) */
+#define QB_FLAG_TC_ONE 32      /* QB_FORM_TC, qb_solve / qb_solve_begin: run one state per
+                                 accumulator where the pair form would be the default (the
+                                 16-bit pair form is the default wherever it applies and no
+                                 tuned entry names the kernel); QB_EINVAL together with
+                                 QB_FLAG_TC_PAIR; the answers are the same */
 #define QB_FLAG_TC_NO16 16     /* QB_FORM_TC: keep the fp32 minima where the 16-bit epilogue
-                                 would apply (tc_kernel 1 instead of 3); the answers are the same */
+                                 would apply (tc_kernel 1 instead of 3, 2 instead of 4); the
+                                 answers are the same */
 #define QB_FLAG_TEST_STALL 2  /* tests only, QB_FORM_TC: the search kernel's tile walk
                                  publishes nothing, so the kernel's bounded waits run out
                                  (about 2 s); the call returns QB_ETIMEOUT and the handle
@@ -139,9 +145,11 @@ typedef struct qb_result {
                              QB_FORM_TC: 15 (the 128 x 256 states of a tile); else 0 */
   int32_t unit_log2;      /* QB_FORM_GRAY: log2 prefix steps per work unit; else 0 */
   int32_t tuned;          /* 1 when qb_autotune's choice for (n, dtype class) was applied */
-  int32_t tc_kernel;      /* QB_FORM_TC: 1 one state per accumulator, fp32 minima; 2 pair form;
-                             3 one state per accumulator, exact 16-bit minima (integer Q whose
-                             accumulator values span fewer than 2^16 integers); 0 other forms */
+  int32_t tc_kernel;      /* QB_FORM_TC: 1 one state per accumulator, fp32 minima; 2 pair form,
+                             fp32 minima; 3 one state per accumulator, exact 16-bit minima
+                             (integer Q whose accumulator values span fewer than 2^16
+                             integers); 4 pair form, exact 16-bit minima (the same, with room
+                             for the pair's per-chunk shifts); 0 other forms */
 } qb_result;
 
 /* Library version (major * 10000 + minor * 100 + patch). */

@@ -232,22 +232,94 @@ def test_tensor_core_16bit_epilogue(cuda_ok, n, hi, seed):
     Q = rng.integers(-hi, hi + 1, (n, n)).astype(np.int32)
     ref = oracle.qbf_port(Q)
     h = _lib.handle(0)
-    r16 = h.solve(Q, form="tc")
+    rd = h.solve(Q, form="tc")
+    r16 = h.solve(Q, form="tc", tc_one=True)
     r32 = h.solve(Q, form="tc", tc_no16=True)
+    # the default is the 16-bit pair form wherever it applies, as here
+    assert rd["plan"]["tc_kernel"] == "pair_u16"
     assert r16["plan"]["tc_kernel"] == "u16" and r32["plan"]["tc_kernel"] == "fp32"
+    for r in (rd, r16, r32):
+        assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
+        assert r["pass1_min"] == ref["best_E"] or (ref["best_E"] == 0 and r["pass1_min"] >= 0)
+    for kw in ({}, {"tc_one": True}):
+        mins = []
+        for s in range(3):
+            mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3, **kw))
+            h.solve_finish(mins[-1], n)
+        outs = []
+        for s in range(3):
+            h.solve_begin(Q, form="tc", shard_index=s, shard_count=3, **kw)
+            outs.append(h.solve_finish(min(mins), n))
+        best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
+        assert best["best_X_int"] == ref["best_X_int"]
+
+
+@pytest.mark.parametrize("n,hi,seed", [(24, 100, 11), (27, 70, 12), (31, 50, 13), (36, 25, 14)])
+def test_tensor_core_pair_16bit_epilogue(cuda_ok, n, hi, seed):
+    """The pair form's 16-bit epilogue (two states per packed accumulator, the partner's value
+    by one add.u16x2 of per-register constants): the oracle's answer and exact pass-1 minimum,
+    the same result as the pair form's fp32 minima, whole problem and five shards (shards start
+    on either sign of the pair's shared variable)."""
+    rng = np.random.default_rng(950 + seed)
+    Q = rng.integers(-hi, hi + 1, (n, n)).astype(np.int32)
+    Q[n - 16, n - 8:] = rng.integers(-hi, hi + 1, 8)  # couplings of the pair's variable with u
+    ref = oracle.qbf_port(Q)
+    h = _lib.handle(0)
+    r16 = h.solve(Q, form="tc", tc_pair=True)
+    r32 = h.solve(Q, form="tc", tc_pair=True, tc_no16=True)
+    assert r16["plan"]["tc_kernel"] == "pair_u16" and r32["plan"]["tc_kernel"] == "pair"
     for r in (r16, r32):
         assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
         assert r["pass1_min"] == ref["best_E"] or (ref["best_E"] == 0 and r["pass1_min"] >= 0)
     mins = []
-    for s in range(3):
-        mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3))
+    for s in range(5):
+        mins.append(h.solve_begin(Q, form="tc", tc_pair=True, shard_index=s, shard_count=5))
         h.solve_finish(mins[-1], n)
+    assert min(mins) == r16["pass1_min"]
     outs = []
-    for s in range(3):
-        h.solve_begin(Q, form="tc", shard_index=s, shard_count=3)
+    for s in range(5):
+        h.solve_begin(Q, form="tc", tc_pair=True, shard_index=s, shard_count=5)
         outs.append(h.solve_finish(min(mins), n))
     best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
     assert best["best_X_int"] == ref["best_X_int"]
+
+
+def test_tensor_core_pair_16bit_shard_minima(cuda_ok):
+    """The pass-1 minimum of every one of 16 shards of the 16-bit pair form equals the fp32
+    pair form's and the one-state form's (all exact on integer Q)."""
+    rng = np.random.default_rng(961)
+    n = 30
+    Q = rng.integers(-60, 61, (n, n)).astype(np.int32)
+    h = _lib.handle(0)
+    for s in range(16):
+        got = []
+        for kw in ({"tc_pair": True}, {"tc_pair": True, "tc_no16": True}, {}):
+            got.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=16, **kw))
+            h.solve_finish(got[-1], n)
+        assert got[0] == got[1] == got[2], (s, got)
+
+
+def test_tensor_core_pair_16bit_needs_room_for_chunk_shifts(cuda_ok):
+    """Accumulator values that span fewer than 2^16 integers, but not with the pair's chunk
+    shifts added (sum of |couplings| of the pair's variable with u bits 5..7): the default is
+    then the one-state 16-bit kernel, the pair form keeps fp32 minima, both exact; the pair
+    and one-state flags together are refused."""
+    n = 24
+    rng = np.random.default_rng(962)
+    Q = np.zeros((n, n), np.int32)
+    for t in range(n - 15):
+        Q[t, n - 8:] = 880  # t-u couplings: span 63,720
+    Q[n - 16, n - 8:n - 5] = 1000  # the pair's variable with u bits 7, 6, 5: shifts of 3000
+    Q[np.arange(n - 8), np.arange(n - 8)] = -rng.integers(0, 2000, n - 8)
+    ref = oracle.qbf_port(Q)
+    h = _lib.handle(0)
+    d = h.solve(Q, form="tc")
+    p = h.solve(Q, form="tc", tc_pair=True)
+    assert d["plan"]["tc_kernel"] == "u16" and p["plan"]["tc_kernel"] == "pair"
+    for r in (d, p):
+        assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
+    with pytest.raises(ValueError):
+        h.solve(Q, form="tc", tc_pair=True, tc_one=True)
 
 
 def test_tensor_core_16bit_epilogue_applies_only_in_range(cuda_ok):
