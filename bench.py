@@ -31,6 +31,9 @@ sys.path.insert(0, ROOT)
 # The pair kernels execute half of it on the tensor pipe (one accumulator per two states).
 FLOPS_PER_STATE_TC = 32
 TC_VARIANTS = {"u16": {"tc_one": True}, "fp32": {"tc_no16": True}, "pair": {"tc_pair": True, "tc_no16": True}}
+# profiling cases: --form name -> tensor-core kernel options
+CASE_FORMS = {"tc_pair": {"tc_pair": True}, "tc_one": {"tc_one": True}, "tc_fp32": {"tc_no16": True},
+              "tc_pair_fp32": {"tc_pair": True, "tc_no16": True}}
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
 
@@ -245,7 +248,7 @@ def bench_ours(args):
         return float(t.item()) / steps, res
 
     form = args.form
-    if form in ("tc_pair", "tc_one"):
+    if form in CASE_FORMS:
         raise SystemExit(f"--form {form} is a profiling case option (--case cfg2 or n36); the headline times it beside tc")
     with ClockSampler(local) as clk:
         ms, res = timed(form, args.steps, args.warmup)
@@ -338,7 +341,7 @@ def bench_case(args):
     32-variable integer QUBO (RandomQUBO seed 0, entries in [-100, 100], symmetric int16);
     n36 = the headline 36-variable TSP QUBO.  Used for ncu captures of a single kernel (a few
     MB on the device).  --form tc runs the tensor-core form's default kernel, tc_pair the pair
-    form, tc_one one state per accumulator."""
+    form, tc_one one state per accumulator, tc_fp32 / tc_pair_fp32 those with fp32 minima."""
     import torch
     import qubo_b200  # noqa: F401
     from qubo_b200 import _lib, configs
@@ -347,7 +350,7 @@ def bench_case(args):
     name = "random_i16_n32" if args.case == "cfg2" else "tsp6_int_n36"
     h = _lib.handle(0)
     stream = torch.cuda.current_stream(0).cuda_stream
-    form, kw = {"tc_pair": ("tc", {"tc_pair": True}), "tc_one": ("tc", {"tc_one": True})}.get(args.form, (args.form, {}))
+    form, kw = ("tc", CASE_FORMS[args.form]) if args.form in CASE_FORMS else (args.form, {})
     for k in range(args.warmup + args.steps):
         r = h.solve(Q, form=form, stream=stream, **kw)
         if k >= args.warmup:
@@ -453,7 +456,7 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto", "tc_pair", "tc_one"])
+    ap.add_argument("--form", default="tc", choices=["tc", "gray", "auto"] + sorted(CASE_FORMS))
     ap.add_argument("--case", default=None, choices=["cfg2", "n36", "batch"],
                     help="cfg2, n36: profiling cases (one line per solve); batch: the 4096-instance batch line")
     args = ap.parse_args()

@@ -12,8 +12,10 @@
 // as a constant operand per register; the 3 high u bits are constant per 32-column chunk
 // and are added to the chunk's minimum).  Every TMEM accumulator thus stands for two
 // states, which halves the MMAs, accumulator round trips and TMEM loads per state, at the
-// price of one fma per derived state in the epilogue.  Measured on B200 (n = 36): 3.9-4.1 ms
-// per 2^36 states, the same as the one-state kernel (3.94 ms); qb_autotune times both.
+// price of one fma per derived state in the epilogue.  Measured on B200 (n = 36 TSP QUBO,
+// 2^36 states): fp32 pair form 4.29 ms, 16-bit pair form (below) 3.20 ms, against 3.93-3.95 ms
+// for one state per accumulator; the 16-bit pair form is the default where it applies, and
+// qb_autotune times both forms.
 //
 // Roles, pipelines, records and bounded waits are those of tc_pass1_kernel<false>
 // (qb_tc.cuh), with "tile" replaced by "pair" in the MMA, B-stage and accumulator
@@ -36,7 +38,10 @@
 // pipe, add.u16x2 at half rate on the FMA pipe, so the partner's adds run beside the
 // minima; per register of 4 states the epilogue spends 2 ALU and 2 FMA issue cycles.  Each
 // warp's pairs share one parity, hence one sign s: one of two copies of the loop.  Constants
-// that differ per chunk (64 per warp) did not stay in registers and ran 25 % slower.
+// that differ per chunk (64 per warp) did not stay in registers and ran 25 % slower; 8
+// epilogue warps over every pair with two register sets each (loads of one pair in flight
+// during the minima of the previous one, 384 threads, 157 registers) ran 4.02 ms, since a
+// stage is then released only after the previous pair's minima.
 //
 // Exactness: for integer Q with sum|Q| <= 2^22, D + s*gamma(u) = y^T V u + C_t'(u) is an
 // integer of magnitude at most sum|Q| (it is the accumulator tile t' would have had), so the
