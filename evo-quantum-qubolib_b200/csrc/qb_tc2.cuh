@@ -8,40 +8,47 @@
 //   gamma(u)    = sum_j W[n-16][n-1-j] u_j          (the couplings of variable n-16 with u)
 //   s           = +1 if t bit 0 is 0, else -1       (bit 0 of gray(i) = (i >> 1) & 1)
 // One MMA computes D for tile t; the epilogue reads each accumulator once and derives the
-// partner tile's value with one fma (gamma of the 5 low u bits is a kernel parameter read
-// as a constant operand per register; the 3 high u bits are constant per 32-column chunk
-// and are added to the chunk's minimum).  Every TMEM accumulator thus stands for two
-// states, which halves the MMAs, accumulator round trips and TMEM loads per state, at the
-// price of one fma per derived state in the epilogue.  Measured on B200 (n = 36 TSP QUBO,
-// 2^36 states): fp32 pair form 4.29 ms, 16-bit pair form (below) 3.20 ms, against 3.93-3.95 ms
-// for one state per accumulator; the 16-bit pair form is the default where it applies, and
-// qb_autotune times both forms.
+// partner tile's value from it.  Every TMEM accumulator thus stands for two states, which
+// halves the MMAs, accumulator round trips and TMEM loads per state.  Measured on B200
+// (n = 36 TSP QUBO, 2^36 states): fp32 pair form 4.29 ms, 16-bit pair form (below) 2.49 ms,
+// against 3.93-3.95 ms for one state per accumulator; the 16-bit pair form is the default
+// where it applies, and qb_autotune times both forms.
 //
 // Roles, pipelines, records and bounded waits are those of tc_pass1_kernel<false>
 // (qb_tc.cuh), with "tile" replaced by "pair" in the MMA, B-stage and accumulator
-// pipelines: per pair the B producer writes the C_t(u) digits of tile t and the row terms of
-// both tiles.  Records: per block of 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in
-// qb_tc.cuh (kGeomTC); a pair never straddles two blocks.
+// pipelines: per pair the B producer writes the column-term digits of tile t and the row
+// terms of both tiles.  acc_full takes two arrivals, the MMA's commit and the MMA thread's
+// own arrive after it saw the pair's B stage full, so the epilogue's acquire of acc_full
+// also orders the row terms and it needs no wait on the B stage.  Records: per block of
+// 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in qb_tc.cuh (kGeomTC); a pair never
+// straddles two blocks.
 //
-// The 16-bit pair form (kU16, tc2_u16_eligible).  As in the one-state 16-bit epilogue
-// (qb_tc.cuh, tc_u16_eligible), the MMA computes F = D + 2^23 - Dmin, whose fp32 pattern
-// holds D - Dmin in its low 16 bits, and the epilogue loads the accumulators two columns per
-// register (.pack::16b, column 2k in the low half of register k of a 32-column chunk).  The
-// partner tile's accumulator D' = D + s * gamma(u) lies in [Dmin, Dmax] as well, so its
-// 16-bit value is (D - Dmin) + s * gamma(u) taken mod 2^16 with no loss.  Per register of a
-// chunk one add.u16x2 of K_s[k] = s * g5(col) + B_s (col = 2k, 2k + 1; the same 16 constants
-// in every chunk, so they stay in registers) and packed 3-input minima give the chunk's
-// partner minimum shifted by B_s - s * ghi(chunk), ghi the gamma of u bits 5..7;
-// B_s = max over the 8 chunks of s * ghi keeps every shifted value in [0, 2^16) when
-// Dmax - Dmin + sum_{b=5..7} |gamma_b| < 2^16, and one add.u16x2 per chunk takes the shift
-// off.  Measured on B200: packed 16-bit minima (2- or 3-input) issue at half rate on the ALU
-// pipe, add.u16x2 at half rate on the FMA pipe, so the partner's adds run beside the
-// minima; per register of 4 states the epilogue spends 2 ALU and 2 FMA issue cycles.  Each
-// warp's pairs share one parity, hence one sign s: one of two copies of the loop.  Constants
-// that differ per chunk (64 per warp) did not stay in registers and ran 25 % slower; 8
-// epilogue warps over every pair with two register sets each (loads of one pair in flight
-// during the minima of the previous one, 384 threads, 157 registers) ran 4.02 ms, since a
-// stage is then released only after the previous pair's minima.
+// fp32 pair form (kU16 = false): the partner's values by one fma per state (gamma of the 5
+// low u bits as constant operands, the 3 high u bits added to each 32-column chunk's minimum)
+// and 3-input fp32 minima.
+//
+// 16-bit pair form (kU16, tc2_u16_eligible).  As in the one-state 16-bit epilogue (qb_tc.cuh,
+// tc_u16_eligible) the accumulator is an integer in [2^23, 2^24) whose fp32 pattern holds a
+// 16-bit value in its low half, loaded two columns per register (.pack::16b).  Here the MMA
+// computes F = D~ + 2^23 - Dlow_s with D~(y, u) = D(y, u) + s * X(u), X the gamma of the chunk
+// bits u4, u5, u6 and Dlow_s = Dmin + min_u s * X(u): the column term carries s * X(u).  In a
+// warp's 64 registers (u = 128 hh + 32 L + 2 j + half, register j of load L) the chunk
+// c = (u4, u5, u6) = (j >> 3, L) and the position k = j & 7 (u1, u2, u3) with the half bit u0
+// index an 8 x 8 grid, and
+//   tile t:   D  - Dmin = (F mod 2^16) - s * X(c) + (Dlow_s - Dmin)       per-chunk correction
+//   tile t':  D' - Dmin = (F mod 2^16) + s * (gamma - X)(k, u0, hh) + (Dlow_s - Dmin)
+//                                                                      per-position correction
+// so tile t takes the packed minimum over each chunk (8 registers) plus one add.u16x2 per
+// chunk, and tile t' the packed minimum over the 8 chunks at each position plus one add.u16x2
+// per position: 64 packed 3-input minimum inputs and 16 adds per 64 registers (8192 states),
+// against 64 adds more when the partner's values are formed register by register.  Every
+// corrected value is D - Dmin of a state, in [0, Dmax - Dmin]; the uncorrected ones lie in
+// [0, Dmax - Dmin + sum_{b=4..6} |gamma_b|] < 2^16 (the eligibility condition), so packed
+// 16-bit minima and mod-2^16 adds are exact.  Each warp's pairs share one parity, hence one
+// sign s and one set of 16 corrections, kept in registers.  The column term's constant part
+// E_U(u) + s X(u) + 2^23 - Dlow_s sits in three constant K slots of each B stage (a stage
+// always holds pairs of one parity); the producer writes only the tile-dependent part
+// T(u) = (t^T W_TU) u as two digits per pair.
 //
 // Exactness: for integer Q with sum|Q| <= 2^22, D + s*gamma(u) = y^T V u + C_t'(u) is an
 // integer of magnitude at most sum|Q| (it is the accumulator tile t' would have had), so the
@@ -65,49 +72,52 @@ struct Tc2Params {
   TcParams P;       // n, nt, gl, stall, exact, inv_scale, W, tile_begin, groups, groups_per_cta, rec, err
   alignas(8) float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
   float whi[3];     // w_5, w_6, w_7: gamma of u bits 5..7 (scaled W)
-  uint32_t k16[2][16];    // 16-bit form: K_s of register k, [0] for s = +1, [1] for s = -1
-  uint32_t corr16[2][8];  // 16-bit form: s * ghi(c) - B_s mod 2^16 in both halves, chunk c = u >> 5
+  // 16-bit form (one sign per accumulator stage: [0] for s = +1, [1] for s = -1)
+  float gx[3];             // gamma of the chunk bits u4, u5, u6
+  float k0s[2];            // 2^23 - Dlow_s, the offset of the column term
+  uint32_t corr_t[2][8];   // tile t: correction of chunk c (u4 = c & 1, u5, u6 = c >> 1), both halves
+  uint32_t corr_p[2][2][8];  // partner: correction of position k (u1..u3) in column half hh (u7)
 };
 
+// u bits that form the 16-bit pair epilogue's chunks (their gamma is folded into the MMA)
+constexpr int kTc2ChunkBits[3] = {4, 5, 6};
+
 // The 16-bit pair form applies (integer Q on the exact path; W unscaled, n x n FP64): the
-// problems of the one-state 16-bit epilogue with room for the chunk shifts,
-// Dmax - Dmin + sum_{b=5..7} |gamma_b| < 2^16.
+// problems of the one-state 16-bit epilogue with room for the chunk offsets,
+// Dmax - Dmin + sum over the chunk bits b of |gamma_b| < 2^16.
 inline bool tc2_u16_eligible(int n, const double* W, float* dmin) {
   double span = 0.0;
   if (!tc_u16_eligible(n, W, dmin, &span)) return false;
-  double ghi = 0.0;
-  for (int b = 5; b < 8; ++b) ghi += std::fabs(W[(size_t)(n - 16) * n + (n - 1 - b)]);
-  return span + ghi <= 65535.0;
+  double gx = 0.0;
+  for (int b : kTc2ChunkBits) gx += std::fabs(W[(size_t)(n - 16) * n + (n - 1 - b)]);
+  return span + gx <= 65535.0;
 }
 
-// the 16-bit pair form's constant tables from gamma (integers on the exact path)
-inline void tc2_u16_tables(const float* gamma, Tc2Params* Q) {
+// the 16-bit pair form's constant tables from gamma (integers on the exact path) and Dmin
+inline void tc2_u16_tables(const float* gamma, float dmin, Tc2Params* Q) {
   int64_t g[8];
   for (int j = 0; j < 8; ++j) g[j] = (int64_t)std::llrint(gamma[j]);
+  for (int b = 0; b < 3; ++b) Q->gx[b] = (float)g[kTc2ChunkBits[b]];
   for (int neg = 0; neg < 2; ++neg) {
     const int64_t s = neg ? -1 : 1;
-    int64_t ghi[8], B = INT64_MIN;
+    int64_t lo = 0;  // min over the chunk bits of s * X(u) = Dlow_s - Dmin
+    for (int b = 0; b < 3; ++b) lo += std::min<int64_t>(0, s * g[kTc2ChunkBits[b]]);
+    Q->k0s[neg] = (float)(8388608.0 - ((double)dmin + (double)lo));
     for (int c = 0; c < 8; ++c) {
-      ghi[c] = 0;
-      for (int b = 0; b < 3; ++b)
-        if ((c >> b) & 1) ghi[c] += g[5 + b];
-      B = std::max(B, s * ghi[c]);
+      const int64_t x = ((c & 1) ? g[4] : 0) + ((c & 2) ? g[5] : 0) + ((c & 4) ? g[6] : 0);
+      const uint32_t v = (uint32_t)((lo - s * x) & 0xffff);
+      Q->corr_t[neg][c] = v | (v << 16);
     }
-    for (int k = 0; k < 16; ++k) {
-      uint32_t h[2];
-      for (int d = 0; d < 2; ++d) {
-        const int col = 2 * k + d;
-        int64_t g5 = 0;
-        for (int b = 0; b < 5; ++b)
-          if ((col >> b) & 1) g5 += g[b];
-        h[d] = (uint32_t)((s * g5 + B) & 0xffff);
+    for (int hh = 0; hh < 2; ++hh)
+      for (int k = 0; k < 8; ++k) {
+        uint32_t h[2];
+        for (int d = 0; d < 2; ++d) {
+          const int64_t gp = (d ? g[0] : 0) + ((k & 1) ? g[1] : 0) + ((k & 2) ? g[2] : 0) + ((k & 4) ? g[3] : 0) +
+                             (hh ? g[7] : 0);
+          h[d] = (uint32_t)((s * gp + lo) & 0xffff);
+        }
+        Q->corr_p[neg][hh][k] = h[0] | (h[1] << 16);
       }
-      Q->k16[neg][k] = h[0] | (h[1] << 16);
-    }
-    for (int c = 0; c < 8; ++c) {
-      const uint32_t v = (uint32_t)((s * ghi[c] - B) & 0xffff);
-      Q->corr16[neg][c] = v | (v << 16);
-    }
   }
 }
 
@@ -151,22 +161,10 @@ __device__ __forceinline__ uint32_t uadd2(uint32_t a, uint32_t b) {
   return d;
 }
 
-// packed unsigned 16-bit minima over the 16 registers of a 32-column chunk (3-input minima)
-__device__ __forceinline__ uint32_t umin16(const uint32_t* r) {
-  const uint32_t a = __vimin3_u16x2(r[0], r[1], r[2]), b = __vimin3_u16x2(r[3], r[4], r[5]);
-  const uint32_t c = __vimin3_u16x2(r[6], r[7], r[8]), d = __vimin3_u16x2(r[9], r[10], r[11]);
-  const uint32_t e = __vimin3_u16x2(r[12], r[13], r[14]);
-  return __vimin3_u16x2(__vimin3_u16x2(a, b, c), __vimin3_u16x2(d, e, r[15]), 0xffffffffu);
-}
-
-// the partner tile's packed minima of one chunk, shifted by B_s - s * ghi(chunk): r + K_s per
-// register (16 constants of the sign, the same in every chunk), then packed minima
-template <int kNeg>
-__device__ __forceinline__ uint32_t umin16_shift(const uint32_t* r, const Tc2Params& Q) {
-  uint32_t v[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) v[k] = uadd2(r[k], Q.k16[kNeg][k]);
-  return umin16(v);
+// packed unsigned 16-bit minimum of 8 registers (3-input minima)
+__device__ __forceinline__ uint32_t umin8(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t e, uint32_t f,
+                                          uint32_t g, uint32_t h) {
+  return __vimin3_u16x2(__vimin3_u16x2(a, b, c), __vimin3_u16x2(d, e, f), umin2(g, h));
 }
 
 template <bool kU16>
@@ -213,7 +211,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       mbar_init(&b_empty[s], 1);
     }
     for (int s = 0; s < kTcStages; ++s) {
-      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_full[s], 2);  // the MMA's commit and the MMA thread (after it saw the B stage full)
       mbar_init(&acc_empty[s], kTcEpiWarps / 2);
     }
     *abort_flag = 0;
@@ -226,12 +224,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
   for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = P.W[i];
   for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
   __syncthreads();
-  // A operand (constant); the 16-bit form as in tc_pass1_kernel<false, true>
+  // A operand (constant)
   for (int e = tid; e < 128 * 16; e += kTcThreads) {
     int y = e >> 4, k = e & 15;
     float v;
-    if (kU16)  // A[y][i] = y_i (i < 7); the column term's digit weights 1, 2048, 32768
-      v = k < 7 ? (float)((y >> k) & 1) : (k == 7 ? 1.0f : (k == 8 ? 2048.0f : (k == 9 ? 32768.0f : 0.0f)));
+    if (kU16)  // A[y][i] = y_i (i < 7); digit weights: T (slots 8, 9) 1, 2048; constant (10-12) 1, 2048, 32768
+      v = k < 7 ? (float)((y >> k) & 1)
+                : (k == 8 || k == 10 ? 1.0f : (k == 9 || k == 11 ? 2048.0f : (k == 12 ? 32768.0f : 0.0f)));
     else if (k < 14)
       v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
     else
@@ -243,7 +242,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
     // one exact fp16 value per coupling row (|(V u)_i| <= 2048), zeros in the unused K slots
     for (int e = tid; e < kTcN * 16; e += kTcThreads) {
       const int u = e >> 4, k = e & 15;
-      if (k >= 7 && k < 10) continue;  // the column term's digits, written per pair
+      if (k >= 8 && k < 13) continue;  // T's digits (per pair) and the constant digits (below)
       double v = 0.0;
       if (k < 7) {
         const double* row = Ws + (n - 9 - k) * n;
@@ -275,6 +274,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
         if ((u >> j2) & 1) e += row[n - 1 - j2];
     }
     EU[u] = (float)e;
+    if (kU16) {
+      // the column term's constant part E_U(u) + s X(u) + 2^23 - Dlow_s in three exact digits;
+      // B stage bs always holds pairs of parity bs & 1, hence one sign
+      const double x = ((u >> 4) & 1 ? (double)Q.gx[0] : 0.0) + ((u >> 5) & 1 ? (double)Q.gx[1] : 0.0) +
+                       ((u >> 6) & 1 ? (double)Q.gx[2] : 0.0);
+      for (int bs = 0; bs < kTcBStages; ++bs) {
+        const uint32_t neg = (uint32_t)(((i_begin >> 1) + (uint64_t)bs) & 1ull);
+        const double c = e + (neg ? -x : x) + (double)Q.k0s[neg];
+        const double d2 = floor(c * (1.0 / 32768.0)), rem = c - 32768.0 * d2;
+        const double d1 = floor(rem * (1.0 / 2048.0)), d0 = rem - 2048.0 * d1;
+        unsigned char* Bst = Bsm + bs * kTcN * 32;
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 10)) = __float2half_rn((float)d0);
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 11)) = __float2half_rn((float)d1);
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 12)) = __float2half_rn((float)d2);
+      }
+    }
   }
   for (int y = tid; y < 128; y += kTcThreads) {
     double e = 0.0;
@@ -395,6 +410,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
           if (p0 + (uint32_t)k >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(k + kTcBStages - kTcStages) % kTcBStages]);
           tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc0 + (uint64_t)(k * (kTcN * 32 / 16)));
           tc_commit(&acc_full[as]);
+          // the second arrival on acc_full: this thread has seen the B stage full, so the
+          // epilogue's acquire of acc_full also orders the row terms written with the stage
+          mbar_arrive(&acc_full[as]);
         }
       }
     }
@@ -410,7 +428,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       ok = mbar_wait(&p_full[sa], (ja >> 6) & 1u, abort_flag) && mbar_wait(&p_full[sb], (jb >> 6) & 1u, abort_flag);
       if (!ok) break;
       __half2 dg[8];
-      __half dl[8];  // 16-bit form: the column term's lowest digit
       float ra[4], rb[4];
       {
         const TcSlot& sl = slots[sa];
@@ -426,13 +443,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
           if (r & 2) cr += f6;
           if (r & 4) cr += f7;
           if (kU16) {
-            // C + 2^23 - Dmin, an integer in [2^23, 2^24): digits d0 < 2048, d1 < 16, d2
-            const float c = EU[lane + 32 * r] + cr + P.k0;
-            const float d2 = floorf(c * (1.0f / 32768.0f));
-            const float rem = c - 32768.0f * d2;
-            const float d1 = floorf(rem * (1.0f / 2048.0f));
-            dl[r] = __float2half_rn(rem - 2048.0f * d1);
-            dg[r] = __halves2half2(__float2half_rn(d1), __float2half_rn(d2));
+            // the tile-dependent part T(u) = (t^T W_TU) u of the column term (an integer,
+            // |T| < 2^22): digits d0 in [0, 2048) and d1 = floor(T / 2048), both exact in fp16
+            const float d1 = floorf(cr * (1.0f / 2048.0f));
+            dg[r] = __floats2half2_rn(fmaf(-2048.0f, d1, cr), d1);
           } else {
             dg[r] = digits(EU[lane + 32 * r] + cr, exact);
           }
@@ -458,10 +472,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       unsigned char* Bst = Bsm + bs * kTcN * 32;
       if (kU16) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          *reinterpret_cast<__half*>(Bst + kmaj_off(lane + 32 * r, 7)) = dl[r];
-          *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
-        }
+        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
       } else {
 #pragma unroll
         for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
@@ -492,59 +503,67 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
       // every pair of this warp has parity sp, so one sign: s = -1 when tile 2p has t bit 0 set
       const uint32_t neg = (uint32_t)(((i_begin >> 1) + sp) & 1ull);
-      uint32_t corr[4];  // chunk shifts of this half (u bits 5, 6 = chunk, bit 7 = hh)
+      uint32_t ct[8], cp[8];  // corrections per chunk (tile 2p) and per position (tile 2p + 1)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) corr[c] = Q.corr16[neg][(hh << 2) | (uint32_t)c];
-      auto pairs = [&](auto kneg) {
-        constexpr int kN = decltype(kneg)::value;
-        uint32_t rec_left = 1u << (gl - 2);
-        uint32_t Jrec = 0;
-        for (uint32_t p = sp; p < npairs && ok; p += 2) {
-          const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-          ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
-          if (!ok) break;
-          const float R1 = Rs[bs * 128 + y] + P.dmin;
-          const float R2 = Rs2[bs * 128 + y] + P.dmin;
-          ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
-          if (!ok) break;
-          tc_fence_after();
-          // the warp's 128 columns at once, two per register; released before the minima
-          uint32_t r[4][16];
-          QB_TC_LD16P(tbase, r[0]);
-          QB_TC_LD16P(tbase + 32, r[1]);
-          QB_TC_LD16P(tbase + 64, r[2]);
-          QB_TC_LD16P(tbase + 96, r[3]);
-          tc_wait_ld();
+      for (int c = 0; c < 8; ++c) {
+        ct[c] = Q.corr_t[neg][c];
+        cp[c] = Q.corr_p[neg][hh][c];
+      }
+      uint32_t rec_left = 1u << (gl - 2);
+      uint32_t Jrec = 0;
+      for (uint32_t p = sp; p < npairs && ok; p += 2) {
+        const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+        // acc_full completes after the MMA thread saw this pair's B stage full: the row terms
+        // written with the stage are visible once it has
+        ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
+        if (!ok) break;
+        tc_fence_after();
+        // the warp's 128 columns at once, two per register; released before the minima.
+        // Register j of load L holds u = 128 hh + 32 L + 2 j + (0 | 1): chunk c = 2 L + (j >> 3)
+        // (u bits 4, 5, 6), position k = j & 7 (u bits 1, 2, 3)
+        uint32_t r[4][16];
+        QB_TC_LD16P(tbase, r[0]);
+        QB_TC_LD16P(tbase + 32, r[1]);
+        QB_TC_LD16P(tbase + 64, r[2]);
+        QB_TC_LD16P(tbase + 96, r[3]);
+        const float R1 = Rs[bs * 128 + y] + P.dmin;
+        const float R2 = Rs2[bs * 128 + y] + P.dmin;
+        tc_wait_ld();
 #pragma unroll
-          for (int c = 0; c < 4; ++c) reg_fence16(r[c]);
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&acc_empty[sp]);
-          // tile 2p: packed minima of D - Dmin; tile 2p + 1: packed minima of the shifted
-          // partner values, unshifted per chunk (mod 2^16, exact: every true value is in range)
-          const uint32_t m1 = umin2(umin2(umin16(r[0]), umin16(r[1])), umin2(umin16(r[2]), umin16(r[3])));
-          const uint32_t m2 = umin2(umin2(uadd2(umin16_shift<kN>(r[0], Q), corr[0]), uadd2(umin16_shift<kN>(r[1], Q), corr[1])),
-                                    umin2(uadd2(umin16_shift<kN>(r[2], Q), corr[2]), uadd2(umin16_shift<kN>(r[3], Q), corr[3])));
-          rmin = fmin3(rmin, (float)min(m1 & 0xffffu, m1 >> 16) + R1, (float)min(m2 & 0xffffu, m2 >> 16) + R2);
-          if (--rec_left == 0) {
-            const float wm = warp_min_f(rmin) * P.inv_scale;
-            if (lane == 0) {
-              float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
-              if (wm >= 0.f)
-                atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
-              else
-                atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
-            }
-            ++Jrec;
-            rec_left = 1u << (gl - 2);
-            rmin = inf;
-          }
+        for (int c = 0; c < 4; ++c) reg_fence16(r[c]);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[sp]);
+        // tile 2p: minimum over each chunk, corrected per chunk; tile 2p + 1: minimum over the
+        // chunks at each position, corrected per position (mod 2^16, exact: every corrected
+        // value is D - Dmin of a state, in [0, 2^16))
+        uint32_t v1[8], v2[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const uint32_t* a = &r[c >> 1][(c & 1) * 8];
+          v1[c] = uadd2(umin8(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]), ct[c]);
         }
-      };
-      if (neg)
-        pairs(std::integral_constant<int, 1>());
-      else
-        pairs(std::integral_constant<int, 0>());
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          v2[k] = uadd2(umin8(r[0][k], r[0][k + 8], r[1][k], r[1][k + 8], r[2][k], r[2][k + 8], r[3][k], r[3][k + 8]),
+                        cp[k]);
+        const uint32_t m1 = umin8(v1[0], v1[1], v1[2], v1[3], v1[4], v1[5], v1[6], v1[7]);
+        const uint32_t m2 = umin8(v2[0], v2[1], v2[2], v2[3], v2[4], v2[5], v2[6], v2[7]);
+        rmin = fmin3(rmin, (float)min(m1 & 0xffffu, m1 >> 16) + R1, (float)min(m2 & 0xffffu, m2 >> 16) + R2);
+        if (--rec_left == 0) {
+          const float wm = warp_min_f(rmin) * P.inv_scale;
+          if (lane == 0) {
+            float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+            if (wm >= 0.f)
+              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+            else
+              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+          }
+          ++Jrec;
+          rec_left = 1u << (gl - 2);
+          rmin = inf;
+        }
+      }
     } else {
       const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
       const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
@@ -558,14 +577,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       uint32_t Jrec = 0;
       for (uint32_t p = sp; p < npairs && ok; p += 2) {
         const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-        ok = mbar_wait(&b_full[bs], (p >> 3) & 1u, abort_flag);
+        // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
+        const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
+        // acc_full completes after the MMA thread saw this pair's B stage full
+        ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
         if (!ok) break;
         const float R1 = Rs[bs * 128 + y];
         const float R2 = Rs2[bs * 128 + y];
-        // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
-        const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
-        ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
-        if (!ok) break;
         tc_fence_after();
         uint32_t ra[32], rb[32];
         QB_TC_LD32(tbase, ra);
@@ -651,8 +669,7 @@ inline int tc2_launch(const TcPlan& p, const float* gamma, float* rec, void* scr
   Q.whi[2] = gamma[7];
   if (p.u16) {
     P.dmin = p.dmin;
-    P.k0 = 8388608.0f - p.dmin;
-    tc2_u16_tables(gamma, &Q);
+    tc2_u16_tables(gamma, p.dmin, &Q);
   }
   const TcSmemLayout L = tc_layout(p.n);
   const size_t smem = std::max<size_t>(L.total + kTcBStages * 128 * 4, 120 * 1024) + 1024;

@@ -256,8 +256,8 @@ def test_tensor_core_16bit_epilogue(cuda_ok, n, hi, seed):
 
 @pytest.mark.parametrize("n,hi,seed", [(24, 100, 11), (27, 70, 12), (31, 50, 13), (36, 25, 14)])
 def test_tensor_core_pair_16bit_epilogue(cuda_ok, n, hi, seed):
-    """The pair form's 16-bit epilogue (two states per packed accumulator, the partner's value
-    by one add.u16x2 of per-register constants): the oracle's answer and exact pass-1 minimum,
+    """The pair form's 16-bit epilogue (two states per packed accumulator: per-chunk minima
+    for the MMA's tile, per-position minima over the chunks for the partner tile): the oracle's answer and exact pass-1 minimum,
     the same result as the pair form's fp32 minima, whole problem and five shards (shards start
     on either sign of the pair's shared variable)."""
     rng = np.random.default_rng(950 + seed)
@@ -301,9 +301,9 @@ def test_tensor_core_pair_16bit_shard_minima(cuda_ok):
 
 def test_tensor_core_pair_16bit_needs_room_for_chunk_shifts(cuda_ok):
     """Accumulator values that span fewer than 2^16 integers, but not with the pair's chunk
-    shifts added (sum of |couplings| of the pair's variable with u bits 5..7): the default is
-    then the one-state 16-bit kernel, the pair form keeps fp32 minima, both exact; the pair
-    and one-state flags together are refused."""
+    offsets added (sum of |couplings| of the pair's variable with u bits 4..6, here 880 + 2 x
+    1000 on a span of 63,720): the default is then the one-state 16-bit kernel, the pair form
+    keeps fp32 minima, both exact; the pair and one-state flags together are refused."""
     n = 24
     rng = np.random.default_rng(962)
     Q = np.zeros((n, n), np.int32)
