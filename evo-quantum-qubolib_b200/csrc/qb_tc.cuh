@@ -211,6 +211,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint of 40 ns: the MMA issuer's wait for a released
+// accumulator stage, where waking promptly matters more than the few extra polls (measured on
+// the pair kernel: 2.49 -> 2.40 ms per 2^36 states)
+__device__ __forceinline__ bool mbar_try_wait_short(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity), "r"(40u)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait with the short hint; the abort flag and the clock are read every 256 polls
+__device__ __forceinline__ bool mbar_wait_short(uint64_t* b, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_wait_short(b, parity)) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait_short(b, parity)) return true;
+    if ((it & 255u) == 0) {
+      if (*abort_flag) return false;
+      if (globaltimer_ns() - t0 > kTcWaitLimitNs) return false;
+    }
+  }
+}
 // bounded wait: false on timeout (or when another role already gave up).  try_wait suspends
 // the warp in hardware until the phase completes or a system-dependent time limit runs out.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag) {

@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
         for (int k = 0; k < kTcBStages; ++k) {
           const uint32_t as = (uint32_t)k & 1u;
           ok = mbar_wait(&b_full[k], pb, abort_flag) &&
-               mbar_wait(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
+               mbar_wait_short(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
           if (!ok) break;
           tc_fence_after();
           if (p0 + (uint32_t)k >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(k + kTcBStages - kTcStages) % kTcBStages]);
