@@ -456,7 +456,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       mbar_init(&b_empty[s], 1);
     }
     for (int s = 0; s < kTcStages; ++s) {
-      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_full[s], 2);  // the MMA's commit and the MMA thread (after it saw the B stage full)
       mbar_init(&acc_empty[s], kTcEpiWarps / 2);  // the 8 warps that read this stage
     }
     *abort_flag = 0;
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
             const uint32_t as = (uint32_t)k & 1u;
             // tile j0 + k: its B stage is full and tile j0 + k - 2 has left accumulator stage as
             ok = mbar_wait(&b_full[k], pb, abort_flag) &&
-                 mbar_wait(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
+                 mbar_wait_short(&acc_empty[as], (((uint32_t)k >> 1) & 1u) ^ 1u, abort_flag);
             if (!ok) break;
             tc_fence_after();
             // every epilogue warp has released tile j-2 (it read that tile's row terms before its
@@ -682,6 +682,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
             // B stage k starts k * 8 KB after stage 0 (descriptor address field in 16-byte units)
             tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc0 + (uint64_t)(k * (kTcN * 32 / 16)));
             tc_commit(&acc_full[as]);  // one commit per MMA
+            // the second arrival on acc_full: this thread has seen the B stage full, so the
+            // epilogue's acquire of acc_full also orders the row terms written with the stage
+            mbar_arrive(&acc_full[as]);
           }
         }
         if (ok && nt32) {  // the last MMA completes before the item's operands can change
@@ -786,13 +789,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pass1_kernel(TcParams P) {
       for (uint32_t jl = sp; jl < nt32 && ok; jl += 2) {
         const uint32_t j = jbase + jl;  // CTA-wide tile counter (jbase is even)
         const uint32_t bs = j & (uint32_t)(kTcBStages - 1);
-        // the B stage of tile j is full: its row terms are written (b_full cannot move on to
-        // tile j + 8 before this warp has released tile j)
-        ok = mbar_wait(&b_full[bs], (j >> 3) & 1u, abort_flag);
-        if (!ok) break;
-        const float R = Rs[bs * 128 + y];
+        // acc_full completes after the MMA thread saw tile j's B stage full, so its row terms
+        // are visible; they stay until this warp has released tile j (the producer rewrites the
+        // stage for tile j + 8 only after MMA j + 2, which waits for that release)
         ok = mbar_wait(&acc_full[sp], (j >> 1) & 1u, abort_flag);
         if (!ok) break;
+        const float R = Rs[bs * 128 + y];
         tc_fence_after();
         if (kU16) {
           // the warp's 128 columns at once, two per register; released before the minima

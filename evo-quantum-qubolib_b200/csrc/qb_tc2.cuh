@@ -10,7 +10,7 @@
 // One MMA computes D for tile t; the epilogue reads each accumulator once and derives the
 // partner tile's value from it.  Every TMEM accumulator thus stands for two states, which
 // halves the MMAs, accumulator round trips and TMEM loads per state.  Measured on B200
-// (n = 36 TSP QUBO, 2^36 states): fp32 pair form 4.29 ms, 16-bit pair form (below) 2.49 ms,
+// (n = 36 TSP QUBO, 2^36 states): fp32 pair form 3.83 ms, 16-bit pair form (below) 2.36 ms,
 // against 3.93-3.95 ms for one state per accumulator; the 16-bit pair form is the default
 // where it applies, and qb_autotune times both forms.
 //
