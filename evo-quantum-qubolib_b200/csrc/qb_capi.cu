@@ -554,10 +554,24 @@ int begin_launch(qb_handle* h, const qb_problem* p, const qb_options* o, Plan& P
     // default kernel where neither a flag nor the tuned entry names one: the 16-bit pair form
     // wherever it applies (the fastest measured), else one state per accumulator
     const qb_handle::Tuned& T = h->tuned[P.is_int ? 1 : 0][P.n];
-    if (!P.tc.pair && P.tc.exact && !no16 && !(o->flags & QB_FLAG_TC_ONE) && T.form != QB_FORM_TC)
-      P.tc.pair = qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin);
-    P.tc.u16 = P.tc.exact && !no16 &&
-               (P.tc.pair ? qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin) : qb::tc_u16_eligible(P.n, W.data(), &P.tc.dmin));
+    // off the exact path (float Q, or integer Q beyond 2^22): the 16-bit pair form on values
+    // rounded to integers in units of 1/sigma, with its error bound, where it applies and the
+    // pair form is the default, requested or tuned
+    double sg = 0.0, qeps = 0.0;
+    float qdmin = 0.f;
+    const bool want_pair = P.tc.pair || (!(o->flags & QB_FLAG_TC_ONE) && T.form != QB_FORM_TC);
+    if (!P.tc.exact && !no16 && want_pair && qb::tc2_u16_quantized(P.n, W.data(), P.abs_sum, &sg, &qdmin, &qeps)) {
+      P.tc.pair = P.tc.u16 = true;
+      P.tc.scale = sg;
+      P.tc.dmin = qdmin;
+      P.tc.eps = P.eps = qeps;
+      for (int j = 0; j < 8; ++j) P.tc.gamma[j] = (float)(W[(size_t)(P.n - 16) * P.n + (P.n - 1 - j)] * sg);
+    } else {
+      if (!P.tc.pair && P.tc.exact && !no16 && !(o->flags & QB_FLAG_TC_ONE) && T.form != QB_FORM_TC)
+        P.tc.pair = qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin);
+      P.tc.u16 = P.tc.exact && !no16 &&
+                 (P.tc.pair ? qb::tc2_u16_eligible(P.n, W.data(), &P.tc.dmin) : qb::tc_u16_eligible(P.n, W.data(), &P.tc.dmin));
+    }
   }
   rc = upload_W(h, W);
   if (rc) return rc;

@@ -93,7 +93,58 @@ inline bool tc2_u16_eligible(int n, const double* W, float* dmin) {
   return span + gx <= 65535.0;
 }
 
-// the 16-bit pair form's constant tables from gamma (integers on the exact path) and Dmin
+// The 16-bit pair form off the exact path (float Q, or integer Q with sum|Q| > 2^22).  The
+// kernel then works in units of 1/sigma, sigma a power of two applied to W: every MMA operand
+// (the y coupling rows, T(u), the column term's constant part, the gammas of the corrections)
+// is rounded to an integer in those units, so the accumulators are integers and the 16-bit
+// epilogue stays exact on the rounded values.  Per state the roundings add at most 4.5 units
+// (seven y rows, T and E_U at 0.5 each), the partner's rounded gammas 4 more, the row term's
+// bias 0.5, plus fp32 rounding of the row terms and of T below 2^-18 sum|Q| sigma; eps =
+// 10 / sigma + 2^-16 sum|Q| bounds it (unscaled) and pass 2 re-walks every record within
+// 2 eps of the minimum in FP64.  Applies when, at the largest such sigma, every y coupling
+// row stays within +-2047 units, the value span with the chunk offsets and a 40-unit margin
+// within 2^16 units, and the span covers at least 1024 units.  W: the unscaled n x n FP64 W.
+// On success: sigma, dmin (the lower bound of the rounded values in units, an integer) and eps.
+inline bool tc2_u16_quantized(int n, const double* W, double abs_sum, double* sigma, float* dmin, double* eps) {
+  if (n < 20) return false;
+  double lo = 0.0, hi = 0.0, rowmax = 0.0;
+  auto add = [&](double w) {
+    if (w < 0) lo += w;
+    else hi += w;
+  };
+  for (int i = 0; i < 7; ++i) {
+    double rp = 0.0, rn = 0.0;
+    for (int j = 0; j < 8; ++j) {
+      const double w = W[(size_t)(n - 9 - i) * n + (n - 1 - j)];
+      if (w < 0) rn -= w;
+      else rp += w;
+      add(w);
+    }
+    rowmax = std::max(rowmax, std::max(rp, rn));
+  }
+  for (int j = 0; j < 8; ++j) {
+    const int a = n - 1 - j;
+    add(W[(size_t)a * n + a]);
+    for (int j2 = 0; j2 < j; ++j2) add(W[(size_t)a * n + (n - 1 - j2)]);
+    for (int t = 0; t < n - 15; ++t) add(W[(size_t)t * n + a]);
+  }
+  double gA = 0.0;
+  for (int b : kTc2ChunkBits) gA += std::fabs(W[(size_t)(n - 16) * n + (n - 1 - b)]);
+  const double span = hi - lo;
+  if (!(span > 0.0) || !std::isfinite(span + gA)) return false;
+  double lim = (65535.0 - 40.0) / (span + gA);
+  if (rowmax > 0.0) lim = std::min(lim, 2047.0 / rowmax);
+  double sg = std::ldexp(1.0, (int)std::floor(std::log2(lim)));
+  while (sg * rowmax > 2047.0 || sg * (span + gA) + 40.0 > 65535.0) sg *= 0.5;
+  if (sg * span < 1024.0) return false;  // too coarse: most records would become candidates
+  *sigma = sg;
+  *dmin = (float)(std::floor(sg * lo) - 12.0);
+  *eps = 10.0 / sg + std::ldexp(abs_sum, -16);
+  return true;
+}
+
+// the 16-bit pair form's constant tables from gamma (integers in the kernel's units, rounded
+// here) and Dmin
 inline void tc2_u16_tables(const float* gamma, float dmin, Tc2Params* Q) {
   int64_t g[8];
   for (int j = 0; j < 8; ++j) g[j] = (int64_t)std::llrint(gamma[j]);
@@ -249,7 +300,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
         for (int j = 0; j < 8; ++j)
           if ((u >> j) & 1) v += row[n - 1 - j];
       }
-      const __half hv = __float2half_rn((float)v);
+      // an integer in the kernel's units (rint: the identity on the exact path)
+      const __half hv = __float2half_rn((float)rint(v));
       for (int s = 0; s < kTcBStages; ++s) *reinterpret_cast<__half*>(Bsm + s * kTcN * 32 + kmaj_off(u, k)) = hv;
     }
   } else {
@@ -281,7 +333,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
                        ((u >> 6) & 1 ? (double)Q.gx[2] : 0.0);
       for (int bs = 0; bs < kTcBStages; ++bs) {
         const uint32_t neg = (uint32_t)(((i_begin >> 1) + (uint64_t)bs) & 1ull);
-        const double c = e + (neg ? -x : x) + (double)Q.k0s[neg];
+        const double c = rint(e) + (neg ? -x : x) + (double)Q.k0s[neg];
         const double d2 = floor(c * (1.0 / 32768.0)), rem = c - 32768.0 * d2;
         const double d1 = floor(rem * (1.0 / 2048.0)), d0 = rem - 2048.0 * d1;
         unsigned char* Bst = Bsm + bs * kTcN * 32;
@@ -443,10 +495,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
           if (r & 2) cr += f6;
           if (r & 4) cr += f7;
           if (kU16) {
-            // the tile-dependent part T(u) = (t^T W_TU) u of the column term (an integer,
-            // |T| < 2^22): digits d0 in [0, 2048) and d1 = floor(T / 2048), both exact in fp16
-            const float d1 = floorf(cr * (1.0f / 2048.0f));
-            dg[r] = __floats2half2_rn(fmaf(-2048.0f, d1, cr), d1);
+            // the tile-dependent part T(u) = (t^T W_TU) u of the column term, rounded to an
+            // integer in the kernel's units (the identity on the exact path), |T| < 2^22: digits
+            // d0 in [0, 2048) and d1 = floor(T / 2048), both exact in fp16
+            const float tq = rintf(cr);
+            const float d1 = floorf(tq * (1.0f / 2048.0f));
+            dg[r] = __floats2half2_rn(fmaf(-2048.0f, d1, tq), d1);
           } else {
             dg[r] = digits(EU[lane + 32 * r] + cr, exact);
           }

@@ -323,7 +323,8 @@ def test_tensor_core_pair_16bit_needs_room_for_chunk_shifts(cuda_ok):
 
 
 def test_tensor_core_16bit_epilogue_applies_only_in_range(cuda_ok):
-    """A coupling row beyond +-2048 or a value span of 2^16 or more keeps the fp32 minima."""
+    """On the exact integer path a coupling row beyond +-2048 or a value span of 2^16 or more
+    keeps the fp32 minima; float Q takes the 16-bit pair form on rounded values."""
     rng = np.random.default_rng(77)
     n = 26
     h = _lib.handle(0)
@@ -336,4 +337,52 @@ def test_tensor_core_16bit_epilogue_applies_only_in_range(cuda_ok):
         ref = oracle.qbf_port(Q)
         assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
     f = h.solve(rng.standard_normal((n, n)), form="tc")
-    assert f["plan"]["tc_kernel"] == "fp32"
+    assert f["plan"]["tc_kernel"] == "pair_u16" and f["err_bound"] > 0
+
+
+@pytest.mark.parametrize("n,seed", [(20, 1), (24, 2), (29, 3), (33, 4), (36, 5)])
+def test_tensor_core_pair_16bit_float(cuda_ok, n, seed):
+    """Float Q in the 16-bit pair form: values rounded to integers in units of a power of two,
+    a stated error bound, every record within twice the bound re-walked in FP64.  The FP64
+    argmin and energy of the oracle (float32 and float64 Q), the same state as the one-state
+    fp32 kernel, whole problem and three shards."""
+    rng = np.random.default_rng(990 + seed)
+    G = rng.standard_normal((n, n))
+    h = _lib.handle(0)
+    for Q in (((G + G.T) / 2).astype(np.float32), G):
+        ref = oracle.qbf_port(Q)
+        r = h.solve(Q, form="tc")
+        assert r["plan"]["tc_kernel"] == "pair_u16" and r["err_bound"] > 0
+        _check(Q, _as_sol(r), ref)
+        one = h.solve(Q, form="tc", tc_one=True)
+        assert one["plan"]["tc_kernel"] == "fp32" and one["best_X_int"] == r["best_X_int"]
+        mins = []
+        for s in range(3):
+            mins.append(h.solve_begin(Q, form="tc", shard_index=s, shard_count=3))
+            h.solve_finish(mins[-1], n)
+        outs = []
+        for s in range(3):
+            h.solve_begin(Q, form="tc", shard_index=s, shard_count=3)
+            outs.append(h.solve_finish(min(mins), n))
+        best = min((o for o in outs if o["found"]), key=lambda o: (o["best_E"], o["order_key"]))
+        assert best["best_X_int"] == ref["best_X_int"]
+
+
+def test_tensor_core_pair_16bit_rounded_integers(cuda_ok):
+    """Integer Q beyond the exact-digit range (sum|Q| > 2^22) takes the 16-bit pair form on
+    rounded values with a nonzero error bound; pass 2 makes the answer bit-exact.  A problem
+    whose u variables have no couplings (a zero value span) keeps one state per accumulator."""
+    rng = np.random.default_rng(995)
+    n = 26
+    Q = rng.integers(-300000, 300001, (n, n)).astype(np.int64)
+    ref = oracle.qbf_port(Q)
+    h = _lib.handle(0)
+    r = h.solve(Q, form="tc")
+    assert r["plan"]["tc_kernel"] == "pair_u16" and r["err_bound"] > 0
+    assert (r["best_X_int"], r["best_E_int"]) == (ref["best_X_int"], ref["best_E"])
+    Z = rng.standard_normal((n, n))
+    Z[:, n - 8:] = 0.0
+    Z[n - 8:, :] = 0.0
+    z = h.solve(Z, form="tc")
+    assert z["plan"]["tc_kernel"] == "fp32"
+    _check(Z, _as_sol(z), oracle.qbf_port(Z))
