@@ -33,6 +33,7 @@ struct BatchInst {
   int A, B;                         // QBF tie rule split (A inverse-Gray ranked prefix bits)
   int natural;                      // 1: natural order (smallest X) among ties
   int is_int;
+  int tc_kernel;                    // tensor-core plan: qb_result.tc_kernel (1 fp32, 4 16-bit pair)
   uint64_t w_off;     // doubles into the packed W array
   uint64_t gtab_off;  // floats into the packed G tables
   uint64_t rec_off;   // floats into the packed record minima

@@ -120,7 +120,7 @@ struct qb_handle_s {
   cudaStream_t own = nullptr;
   cudaStream_t st = nullptr;
   DevBuf W, gtab, rec, cand, misc, exout, tcscratch;
-  DevBuf bat[14];  // qb_solve_batch: W, insts, gtab items, unit items, selection ids, cands, out, G tables,
+  DevBuf bat[15];  // qb_solve_batch: W, insts, gtab items, unit items, selection ids, cands, out, G tables,
                    // records, minima, scaled W, tensor-core items, item ranges, error word
   HostBuf hW, hmisc, hout, hbat;  // hbat: qb_solve_batch's packed W matrices (pinned)
   HostBuf hstage;                  // qb_solve_batch: descriptors and work lists (pinned)
@@ -1221,6 +1221,46 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     }
     sm_exact = std::max(sm_exact, qb::exact_smem_bytes(n, free_bits));
   }
+  // The 16-bit pair kernel for the tensor-core problems when every one of them takes it: exact
+  // integer digits with 16-bit room, else values rounded to a power-of-two unit with an error
+  // bound (tc2_u16_quantized).  Its unit replaces the problem's W scale and its bound the
+  // problem's eps; each problem gets a table of its 16-bit constants.
+  std::vector<qb::Tc2Tab> tc_tabs;
+  bool tc_pair = !tcs.empty() && !(o->flags & (QB_FLAG_TC_ONE | QB_FLAG_TC_NO16));
+  if (tc_pair) {
+    tc_tabs.resize(tcs.size());
+    std::vector<double> sg(tcs.size(), 1.0), ep(tcs.size(), 0.0);
+    for (size_t k = 0; k < tcs.size() && tc_pair; ++k) {
+      const int j = tcs[k].first;
+      const int n = insts[j].n;
+      const double* W = Wall + w_offs[j];
+      float dm = 0.f;
+      const bool fits = (insts[j].exact_digits && qb::tc2_u16_eligible(n, W, &dm)) ||
+                        qb::tc2_u16_quantized(n, W, sums[j], &sg[k], &dm, &ep[k]);
+      if (!fits) {
+        tc_pair = false;
+        break;
+      }
+      if (!(insts[j].exact_digits && ep[k] == 0.0 && sg[k] == 1.0)) insts[j].exact_digits = 0;
+      float gamma[8];
+      for (int b = 0; b < 8; ++b) gamma[b] = (float)(W[(size_t)(n - 16) * n + (n - 1 - b)] * sg[k]);
+      qb::tc2_u16_tables(gamma, dm, &tc_tabs[k]);
+      tc_tabs[k].dmin = dm;
+    }
+    if (tc_pair) {
+      for (size_t k = 0; k < tcs.size(); ++k) {
+        qb::BatchInst& I = insts[tcs[k].first];
+        I.scale = sg[k];
+        I.eps = ep[k];
+        I.tc_kernel = 4;
+        tc_scale[k].second = sg[k];
+      }
+    } else {
+      tc_tabs.clear();
+    }
+  }
+  for (auto& t : tcs)
+    if (!insts[t.first].tc_kernel) insts[t.first].tc_kernel = 1;
   // the tensor-core problems' W scaled into their own block (several threads)
   parallel_ranges((int)tcs.size(), [&](int k0, int k1) {
     for (int k = k0; k < k1; ++k) {
@@ -1240,6 +1280,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   // the tensor-core problems' record blocks, dealt out as contiguous runs to one persistent
   // CTA per SM (a run may span problems: one item per problem piece)
   std::vector<qb::TcItem> items;
+  std::vector<qb::Tc2Tab> item_tabs;                 // the 16-bit pair kernel: per item
   std::vector<std::pair<uint64_t, uint64_t>> offs;  // (scaled-W offset, record offset) per item
   std::vector<uint32_t> first(1, 0);
   if (!tcs.empty()) {
@@ -1248,7 +1289,8 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     const uint64_t ctas = std::min<uint64_t>((uint64_t)h->sm_count, total);
     const uint64_t per = (total + ctas - 1) / ctas;
     uint64_t left = per;
-    for (auto& t : tcs) {
+    for (size_t k = 0; k < tcs.size(); ++k) {
+      const auto& t = tcs[k];
       const qb::BatchInst& I = insts[t.first];
       const uint64_t groups = 1ull << (I.n - 15 - I.gl);
       uint64_t g = 0;
@@ -1263,6 +1305,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
         it.exact = I.exact_digits;
         it.inv_scale = (float)(1.0 / I.scale);
         items.push_back(it);
+        if (tc_pair) item_tabs.push_back(tc_tabs[k]);
         g += take;
         left -= take;
         if (left == 0) {
@@ -1292,6 +1335,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     if ((rc = ensure_for(B[11], items))) return rc;
     if ((rc = ensure_for(B[12], first))) return rc;
     QB_CUDA(B[13].ensure(16));
+    if (tc_pair && (rc = ensure_for(B[14], item_tabs))) return rc;
   }
   QB_CUDA(h->hout.ensure(res_bytes + 16));
   uint64_t* emin = static_cast<uint64_t*>(B[9].p);
@@ -1312,6 +1356,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
   if (!tcs.empty()) {
     stg.add(B[11].p, items);
     stg.add(B[12].p, first);
+    if (tc_pair) stg.add(B[14].p, item_tabs);
   }
   QB_CUDA(h->hstage.ensure(std::max<size_t>(stg.bytes.size(), 16)));
   memcpy(h->hstage.p, stg.bytes.data(), stg.bytes.size());
@@ -1331,8 +1376,13 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     P.n_max = n_tc_max;
     P.err = tc_err;
     const qb::TcSmemLayout L = qb::tc_layout(n_tc_max);
-    sm_tc = std::max<size_t>(L.total, 120 * 1024) + 1024;
-    QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
+    if (tc_pair) {  // plus the second tile's row terms of each B stage
+      sm_tc = std::max<size_t>(L.total + qb::kTcBStages * 128 * 4, 120 * 1024) + 1024;
+      QB_CUDA(cudaFuncSetAttribute(qb::tc_pair_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
+    } else {
+      sm_tc = std::max<size_t>(L.total, 120 * 1024) + 1024;
+      QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
+    }
   }
   if (any_gray) {
     QB_CUDA(cudaFuncSetAttribute(qb::batch_gtab_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_gtab));
@@ -1363,7 +1413,11 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     if (!tcs.empty()) {
       QB_CUDA(cudaMemcpyAsync(B[10].p, Wtc, wtc_used * sizeof(double), cudaMemcpyHostToDevice, st));
       QB_CUDA(cudaMemsetAsync(tc_err, 0, 16, st));
-      qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(P);
+      if (tc_pair)
+        qb::tc_pair_items_kernel<<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(
+            P, static_cast<const qb::Tc2Tab*>(B[14].p));
+      else
+        qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(P);
       ++h->kernels;
     }
     if (timed) {
@@ -1396,7 +1450,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     std::vector<uint64_t> key = {(uint64_t)m, (uint64_t)w_used, (uint64_t)wtc_used, (uint64_t)cap,
                                  (uint64_t)gitems.size(), (uint64_t)uitems.size(), (uint64_t)gray_ids.size(),
                                  (uint64_t)first.size(), (uint64_t)sm_gtab, (uint64_t)sm_gray, (uint64_t)sm_exact,
-                                 (uint64_t)sm_tc, (uint64_t)any_gray, (uint64_t)(uintptr_t)Wall,
+                                 (uint64_t)sm_tc, (uint64_t)any_gray, (uint64_t)tc_pair, (uint64_t)(uintptr_t)Wall,
                                  (uint64_t)(uintptr_t)h->hstage.p, (uint64_t)(uintptr_t)h->hout.p,
                                  (uint64_t)(uintptr_t)h->own};
     for (int k = 0; k < 14; ++k) key.push_back((uint64_t)(uintptr_t)B[k].p);
@@ -1489,7 +1543,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     } else if (I.kind == qb::kBatchTC) {
       R.rec_log2 = I.gl;
       R.suffix_bits = 15;
-      R.tc_kernel = 1;  // the batch's tensor-core items take fp32 minima
+      R.tc_kernel = I.tc_kernel;  // 4: the 16-bit pair kernel, 1: one state with fp32 minima
       R.tuned = (T.tc_gl || T.form == QB_FORM_TC) ? 1 : 0;
     } else {
       R.rec_log2 = I.fbits;

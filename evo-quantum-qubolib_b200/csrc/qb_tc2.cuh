@@ -143,9 +143,20 @@ inline bool tc2_u16_quantized(int n, const double* W, double abs_sum, double* si
   return true;
 }
 
+// per-item constants of the batched 16-bit pair kernel (tc_pair_items_kernel): those of
+// Tc2Params for the item's problem, and its Dmin
+struct Tc2Tab {
+  float gx[3];
+  float k0s[2];
+  float dmin;
+  uint32_t corr_t[2][8];
+  uint32_t corr_p[2][2][8];
+};
+
 // the 16-bit pair form's constant tables from gamma (integers in the kernel's units, rounded
-// here) and Dmin
-inline void tc2_u16_tables(const float* gamma, float dmin, Tc2Params* Q) {
+// here) and Dmin, into Tc2Params or Tc2Tab
+template <class Tab>
+inline void tc2_u16_tables(const float* gamma, float dmin, Tab* Q) {
   int64_t g[8];
   for (int j = 0; j < 8; ++j) g[j] = (int64_t)std::llrint(gamma[j]);
   for (int b = 0; b < 3; ++b) Q->gx[b] = (float)g[kTc2ChunkBits[b]];
@@ -693,6 +704,408 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
   if (!ok) {
     *abort_flag = 1;
     atomicOr(P.err, kErrTimeout);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+  }
+}
+
+// The batched 16-bit pair kernel: tc_pair_kernel<true> over a list of work items (runs of
+// record blocks of the batch's problems, qb_batch.cuh), as tc_pass1_kernel<true> does for one
+// state per accumulator.  Every role walks the CTA's tiles in the same order; barrier slots,
+// B stages and phases follow the CTA-wide tile counter jbase (a multiple of 32: every item has
+// a multiple of 2^gl >= 32 tiles), pairs the pair counter jbase / 2.  Between items all roles
+// meet at a CTA barrier with the pipelines empty (the MMA thread waits for its last MMA), so
+// the per-item tables, B operand columns and constants can be rewritten.  tabs[it] holds the
+// 16-bit constants of item it's problem; its W is in the item's units (scaled by sigma).
+__global__ void __launch_bounds__(kTcThreads, 1)
+tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restrict__ tabs) {
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const TcSmemLayout L = tc_layout(P.n_max);  // only the W block grows with n
+  unsigned char* Asm = tc_smem + L.a_off;
+  unsigned char* Bsm = tc_smem + L.b_off;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + L.bar_off);
+  uint64_t* p_full = bars;
+  uint64_t* p_empty = p_full + kTcParamSlots;
+  uint64_t* b_full = p_empty + kTcParamSlots;
+  uint64_t* b_empty = b_full + kTcBStages;
+  uint64_t* acc_full = b_empty + kTcBStages;
+  uint64_t* acc_empty = acc_full + kTcStages;
+  TcSlot* slots = reinterpret_cast<TcSlot*>(tc_smem + L.slot_off);
+  float* EU = reinterpret_cast<float*>(tc_smem + L.eu_off);
+  float* EY = reinterpret_cast<float*>(tc_smem + L.ey_off);
+  float* Rs = reinterpret_cast<float*>(tc_smem + L.rs_off);  // tile t of each pair
+  float* Rs2 = reinterpret_cast<float*>(tc_smem + L.total);  // tile t' of each pair
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + L.misc_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tc_smem + L.misc_off + 4);
+  double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
+  double* Ws = reinterpret_cast<double*>(tc_smem + L.w_off);
+
+  const uint32_t it_lo = P.item_first[blockIdx.x], it_hi = P.item_first[blockIdx.x + 1];
+  if (it_lo >= it_hi) return;  // uniform per CTA
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcParamSlots; ++s) {
+      mbar_init(&p_full[s], 1);
+      mbar_init(&p_empty[s], 1);
+    }
+    for (int s = 0; s < kTcBStages; ++s) {
+      mbar_init(&b_full[s], 1);
+      mbar_init(&b_empty[s], 1);
+    }
+    for (int s = 0; s < kTcStages; ++s) {
+      mbar_init(&acc_full[s], 2);  // the MMA's commit and the MMA thread (after it saw the B stage full)
+      mbar_init(&acc_empty[s], kTcEpiWarps / 2);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  // A operand (constant, the same for every item): A[y][i] = y_i (i < 7); digit weights: T
+  // (slots 8, 9) 1, 2048; the constant part (slots 10-12) 1, 2048, 32768
+  for (int e = tid; e < 128 * 16; e += kTcThreads) {
+    const int y = e >> 4, k = e & 15;
+    const float v = k < 7 ? (float)((y >> k) & 1)
+                          : (k == 8 || k == 10 ? 1.0f : (k == 9 || k == 11 ? 2048.0f : (k == 12 ? 32768.0f : 0.0f)));
+    *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  uint32_t jbase = 0;  // CTA-wide tile counter
+  for (uint32_t it = it_lo; it < it_hi; ++it) {
+    const TcItem I = P.items[it];
+    const Tc2Tab& Tb = tabs[it];
+    const int n = I.n, nt = n - 15, gl = I.gl;
+    const uint64_t i_begin = I.i_begin, ntiles = I.ntiles;
+    float* rec = I.rec;
+    const uint64_t t0 = gray64(i_begin);
+    const uint32_t pbase = jbase >> 1;  // CTA-wide pair counter (a multiple of 16)
+
+    // ------------------------------------------------------------ per-item set-up
+    for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = I.W[i];
+    for (uint64_t r = (uint64_t)tid; r < ((ntiles >> gl) << 3); r += kTcThreads) rec[r] = __int_as_float(0x7f800000);
+    __syncthreads();
+    // B operand: coupling rows of the y variables (one exact fp16 integer each), zeros
+    for (int e = tid; e < kTcN * 16; e += kTcThreads) {
+      const int u = e >> 4, k = e & 15;
+      if (k >= 8 && k < 13) continue;  // T's digits (per pair) and the constant digits (below)
+      double v = 0.0;
+      if (k < 7) {
+        const double* row = Ws + (n - 9 - k) * n;
+        for (int j = 0; j < 8; ++j)
+          if ((u >> j) & 1) v += row[n - 1 - j];
+      }
+      const __half hv = __float2half_rn((float)rint(v));
+      for (int s = 0; s < kTcBStages; ++s) *reinterpret_cast<__half*>(Bsm + s * kTcN * 32 + kmaj_off(u, k)) = hv;
+    }
+    for (int u = tid; u < kTcN; u += kTcThreads) {
+      double e = 0.0;
+      for (int j = 0; j < 8; ++j) {
+        if (!((u >> j) & 1)) continue;
+        const double* row = Ws + (n - 1 - j) * n;
+        e += row[n - 1 - j];
+        for (int j2 = 0; j2 < j; ++j2)
+          if ((u >> j2) & 1) e += row[n - 1 - j2];
+      }
+      EU[u] = (float)e;
+      // the column term's constant part E_U(u) + s X(u) + 2^23 - Dlow_s in three exact digits;
+      // B stage bs holds pairs of parity bs & 1 (the pair counter is a multiple of 16), one sign
+      const double x = ((u >> 4) & 1 ? (double)Tb.gx[0] : 0.0) + ((u >> 5) & 1 ? (double)Tb.gx[1] : 0.0) +
+                       ((u >> 6) & 1 ? (double)Tb.gx[2] : 0.0);
+      for (int bs = 0; bs < kTcBStages; ++bs) {
+        const uint32_t neg = (uint32_t)(((i_begin >> 1) + (uint64_t)bs) & 1ull);
+        const double c = rint(e) + (neg ? -x : x) + (double)Tb.k0s[neg];
+        const double d2 = floor(c * (1.0 / 32768.0)), rem = c - 32768.0 * d2;
+        const double d1 = floor(rem * (1.0 / 2048.0)), d0 = rem - 2048.0 * d1;
+        unsigned char* Bst = Bsm + bs * kTcN * 32;
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 10)) = __float2half_rn((float)d0);
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 11)) = __float2half_rn((float)d1);
+        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 12)) = __float2half_rn((float)d2);
+      }
+    }
+    for (int y = tid; y < 128; y += kTcThreads) {
+      double e = 0.0;
+      for (int i = 0; i < 7; ++i) {
+        if (!((y >> i) & 1)) continue;
+        const double* row = Ws + (n - 9 - i) * n;
+        e += row[n - 9 - i];
+        for (int i2 = 0; i2 < i; ++i2)
+          if ((y >> i2) & 1) e += row[n - 9 - i2];
+      }
+      EY[y] = (float)e;
+    }
+    for (int e = tid; e < 32 * 16; e += kTcThreads) {
+      const int p = e >> 4, c = e & 15;
+      double v = 0.0;
+      if (c == 15) {
+        for (int k = 0; k < 5; ++k) {
+          if (!((p >> k) & 1)) continue;
+          const double* row = Ws + (n - 16 - k) * n;
+          v += row[n - 16 - k];
+          for (int k2 = 0; k2 < k; ++k2)
+            if ((p >> k2) & 1) v += row[n - 16 - k2];
+        }
+      } else {
+        const int col = c < 8 ? n - 1 - c : n - 9 - (c - 8);
+        for (int k = 0; k < 5; ++k)
+          if ((p >> k) & 1) v += Ws[(n - 16 - k) * n + col];
+      }
+      LO[e] = v;
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t npairs = (uint32_t)(ntiles >> 1);
+
+    bool ok = true;
+    if (warp == 0) {
+      // ---------------------------------------------------------- tile walk (every tile)
+      const int nh = nt - 5;
+      double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) fh[k] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 7; ++k) gh[k] = 0.0;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) c[k] = 0.0;
+      const uint64_t th0 = t0 >> 5;
+      for (int m = 0; m < nh; ++m) {
+        if (!((th0 >> m) & 1)) continue;
+        const double* row = Ws + (n - 21 - m) * n;
+        eh += row[n - 21 - m];
+        for (int m2 = 0; m2 < m; ++m2)
+          if ((th0 >> m2) & 1) eh += row[n - 21 - m2];
+        if (lane < nh && lane != m) h0 += row[n - 21 - lane];
+        if (lane + 32 < nh && lane + 32 != m) h1 += row[n - 21 - lane - 32];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) fh[k] += row[n - 1 - k];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) gh[k] += row[n - 9 - k];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) c[k] += row[n - 16 - k];
+      }
+      for (uint64_t j0 = 0; j0 < ntiles && ok; j0 += 32) {
+        const uint64_t i0 = i_begin + j0;
+        if (j0 > 0) {
+          const int kb = __ffsll((long long)i0) - 1;
+          const int m = kb - 5;
+          const double sg = ((gray64(i0) >> kb) & 1) ? 1.0 : -1.0;
+          const double hm = __shfl_sync(0xffffffffu, m < 32 ? h0 : h1, m & 31);
+          const double* row = Ws + (n - 21 - m) * n;
+          eh += sg * (row[n - 21 - m] + hm);
+          if (lane < nh && lane != m) h0 += sg * row[n - 21 - lane];
+          if (lane + 32 < nh && lane + 32 != m) h1 += sg * row[n - 21 - lane - 32];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) fh[k] += sg * row[n - 1 - k];
+#pragma unroll
+          for (int k = 0; k < 7; ++k) gh[k] += sg * row[n - 9 - k];
+#pragma unroll
+          for (int k = 0; k < 5; ++k) c[k] += sg * row[n - 16 - k];
+        }
+        const uint64_t jg = jbase + j0 + (uint64_t)lane;  // CTA-wide tile counter
+        const int tl = (int)(gray64(i0 + (uint64_t)lane) & 31ull);
+        const double* lo = LO + tl * 16;
+        double et = eh + lo[15];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if ((tl >> k) & 1) et += c[k];
+        const int s = (int)(jg % kTcParamSlots);
+        ok = mbar_wait(&p_empty[s], (uint32_t)(((jg / kTcParamSlots) & 1) ^ 1), abort_flag);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        TcSlot& sl = slots[s];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sl.f[k] = (float)(fh[k] + lo[k]);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) sl.g[k] = (float)(gh[k] + lo[8 + k]);
+        sl.et = (float)et;
+        mbar_arrive(&p_full[s]);
+      }
+    } else if (warp == 1) {
+      // ---------------------------------------------------------- MMA issue (one per pair)
+      if (lane == 0) {
+        const uint64_t adesc = umma_desc(smem_u32(Asm), 128, 256);
+        const uint64_t bdesc0 = umma_desc(smem_u32(Bsm), 128, 256);
+        for (uint32_t p0 = 0; p0 < npairs && ok; p0 += kTcBStages) {
+          const uint32_t g0p = pbase + p0;  // a multiple of 8
+          const uint32_t pb = (g0p >> 3) & 1u;
+#pragma unroll
+          for (int k = 0; k < kTcBStages; ++k) {
+            const uint32_t as = (uint32_t)k & 1u;
+            ok = mbar_wait(&b_full[k], pb, abort_flag) &&
+                 mbar_wait_short(&acc_empty[as], (((g0p + (uint32_t)k) >> 1) & 1u) ^ 1u, abort_flag);
+            if (!ok) break;
+            tc_fence_after();
+            if (g0p + (uint32_t)k >= (uint32_t)kTcStages) mbar_arrive(&b_empty[(k + kTcBStages - kTcStages) % kTcBStages]);
+            tc_mma(tmem + as * (uint32_t)kTcN, adesc, bdesc0 + (uint64_t)(k * (kTcN * 32 / 16)));
+            tc_commit(&acc_full[as]);
+            mbar_arrive(&acc_full[as]);
+          }
+        }
+        if (ok && npairs) {  // the last MMA completes before the item's operands can change
+          const uint32_t pl = pbase + npairs - 1;
+          ok = mbar_wait(&acc_full[pl & 1u], (pl >> 1) & 1u, abort_flag);
+        }
+      }
+      __syncwarp();
+    } else if (warp < 4) {
+      // ---------------------------------------------------------- B producers (per pair)
+      for (uint32_t p = (uint32_t)(warp - 2); p < npairs && ok; p += 2) {
+        const uint32_t pg = pbase + p;
+        const uint32_t ja = jbase + 2 * p, jb = ja + 1;
+        const uint32_t sa = ja & (uint32_t)(kTcParamSlots - 1), sb = jb & (uint32_t)(kTcParamSlots - 1);
+        const uint32_t bs = pg & (uint32_t)(kTcBStages - 1);
+        ok = mbar_wait(&p_full[sa], (ja >> 6) & 1u, abort_flag) && mbar_wait(&p_full[sb], (jb >> 6) & 1u, abort_flag);
+        if (!ok) break;
+        __half2 dg[8];
+        float ra[4], rb[4];
+        {
+          const TcSlot& sl = slots[sa];
+          float s5 = 0.f;
+#pragma unroll
+          for (int jb5 = 0; jb5 < 5; ++jb5)
+            if ((lane >> jb5) & 1) s5 += sl.f[jb5];
+          const float f5 = sl.f[5], f6 = sl.f[6], f7 = sl.f[7];
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            float cr = s5;
+            if (r & 1) cr += f5;
+            if (r & 2) cr += f6;
+            if (r & 4) cr += f7;
+            const float tq = rintf(cr);
+            const float d1 = floorf(tq * (1.0f / 2048.0f));
+            dg[r] = __floats2half2_rn(fmaf(-2048.0f, d1, tq), d1);
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const TcSlot& sl = slots[h ? sb : sa];
+          float g5 = sl.et;
+#pragma unroll
+          for (int i = 0; i < 5; ++i)
+            if ((lane >> i) & 1) g5 += sl.g[i];
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            float v = g5;
+            if (r & 1) v += sl.g[5];
+            if (r & 2) v += sl.g[6];
+            (h ? rb : ra)[r] = v + EY[lane + 32 * r];
+          }
+        }
+        ok = mbar_wait(&b_empty[bs], ((pg >> 3) & 1u) ^ 1u, abort_flag);
+        if (!ok) break;
+        unsigned char* Bst = Bsm + bs * kTcN * 32;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          Rs[bs * 128 + lane + 32 * r] = ra[r];
+          Rs2[bs * 128 + lane + 32 * r] = rb[r];
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&b_full[bs]);
+          mbar_arrive(&p_empty[sa]);
+          mbar_arrive(&p_empty[sb]);
+        }
+      }
+    } else {
+      // ---------------------------------------------------------- epilogue (16-bit minima)
+      const int q = warp & 3;
+      const int cq = (warp - 4) >> 2;
+      const int y = q * 32 + lane;
+      const float inf = __int_as_float(0x7f800000);
+      const uint32_t sp = (uint32_t)cq >> 1;  // pair parity = accumulator stage
+      const uint32_t hh = (uint32_t)cq & 1u;  // column half: u bit 7
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+      const uint32_t neg = (uint32_t)(((i_begin >> 1) + sp) & 1ull);
+      uint32_t ct[8], cp[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        ct[c] = Tb.corr_t[neg][c];
+        cp[c] = Tb.corr_p[neg][hh][c];
+      }
+      const float rbias = Tb.dmin - 8388608.0f;
+      const float inv = I.inv_scale;
+      float rmin = inf;
+      auto pair_step = [&](uint32_t p) -> bool {
+        const uint32_t pg = pbase + p;
+        const uint32_t bs = pg & (uint32_t)(kTcBStages - 1);
+        if (!mbar_wait(&acc_full[sp], (pg >> 1) & 1u, abort_flag)) return false;
+        tc_fence_after();
+        uint32_t r[4][16];
+        QB_TC_LD16P(tbase, r[0]);
+        QB_TC_LD16P(tbase + 32, r[1]);
+        QB_TC_LD16P(tbase + 64, r[2]);
+        QB_TC_LD16P(tbase + 96, r[3]);
+        const float R1 = Rs[bs * 128 + y] + rbias;
+        const float R2 = Rs2[bs * 128 + y] + rbias;
+        tc_wait_ld();
+#pragma unroll
+        for (int c = 0; c < 4; ++c) reg_fence16(r[c]);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[sp]);
+        uint32_t v1[8], v2[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const uint32_t* a = &r[c >> 1][(c & 1) * 8];
+          v1[c] = uadd2(umin8(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]), ct[c]);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          v2[k] = uadd2(umin8(r[0][k], r[0][k + 8], r[1][k], r[1][k + 8], r[2][k], r[2][k + 8], r[3][k], r[3][k + 8]),
+                        cp[k]);
+        const uint32_t m1 = umin8(v1[0], v1[1], v1[2], v1[3], v1[4], v1[5], v1[6], v1[7]);
+        const uint32_t m2 = umin8(v2[0], v2[1], v2[2], v2[3], v2[4], v2[5], v2[6], v2[7]);
+        const float a1 = fminf(__uint_as_float(__byte_perm(m1, 0x4B000000u, 0x7610)),
+                               __uint_as_float(__byte_perm(m1, 0x4B000000u, 0x7632)));
+        const float a2 = fminf(__uint_as_float(__byte_perm(m2, 0x4B000000u, 0x7610)),
+                               __uint_as_float(__byte_perm(m2, 0x4B000000u, 0x7632)));
+        rmin = fmin3(rmin, a1 + R1, a2 + R2);
+        return true;
+      };
+      uint32_t rec_left = 1u << (gl - 2);
+      uint32_t Jrec = 0;
+      for (uint32_t p = sp; p < npairs && ok; p += 4) {
+        ok = pair_step(p) && pair_step(p + 2);
+        if (!ok) break;
+        rec_left -= 2;
+        if (rec_left == 0) {
+          const float wm = warp_min_f(rmin) * inv;
+          if (lane == 0) {
+            float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+            if (wm >= 0.f)
+              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+            else
+              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
+          }
+          ++Jrec;
+          rec_left = 1u << (gl - 2);
+          rmin = inf;
+        }
+      }
+    }
+    if (!ok) {
+      *abort_flag = 1;
+      atomicOr(P.err, kErrTimeout);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    jbase += (uint32_t)ntiles;
+    if (*abort_flag) break;  // uniform: read after the barrier
   }
   tc_fence_before();
   __syncthreads();

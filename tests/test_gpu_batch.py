@@ -124,6 +124,31 @@ def test_batch_tensor_core_members_beyond_exact_digits(cuda_ok):
         _check(Q, r)
 
 
+def test_batch_tensor_core_members_take_the_16bit_pair_kernel(cuda_ok):
+    """When every tensor-core member (n >= 24) fits it, the batch runs the batched 16-bit pair
+    kernel: float members on values rounded to a power-of-two unit with an error bound,
+    integer members on exact digits; the oracle's answers, and the same states as the
+    one-state kernel (QB_FLAG_TC_ONE); an integer member whose values span more than 2^16
+    takes rounded values too and stays exact."""
+    rng = np.random.default_rng(31)
+    Qs = [configs.batch_instance(i) for i in range(0, 4096, 97)]
+    Qs += [rng.integers(-40, 41, (n, n)).astype(np.int32) for n in (24, 27, 29)]
+    h = _lib.handle(0)
+    res = h.solve_batch(Qs)
+    one = h.solve_batch(Qs, tc_one=True)
+    for Q, r, r1 in zip(Qs, res, one):
+        _check(Q, r)
+        assert r1["best_X_int"] == r["best_X_int"]
+        if r["form"] == "tc":
+            assert r["plan"]["tc_kernel"] == "pair_u16" and r1["plan"]["tc_kernel"] == "fp32"
+            assert (r["err_bound"] > 0) == (not np.issubdtype(Q.dtype, np.integer))
+    assert sum(r["form"] == "tc" for r in res) >= 10
+    wide = rng.integers(-2000, 2001, (26, 26)).astype(np.int32)  # exact digits, span beyond 2^16
+    mix = h.solve_batch([Qs[0], wide])
+    for Q, r in zip([Qs[0], wide], mix):
+        _check(Q, r)
+
+
 def _same_shapes(Qs, seed):
     """New matrices with the sizes and dtypes of Qs (the same batch shape, other values)."""
     rng = np.random.default_rng(seed)
