@@ -34,6 +34,8 @@ TC_VARIANTS = {"u16": {"tc_one": True}, "fp32": {"tc_no16": True}, "pair": {"tc_
 # profiling cases: --form name -> tensor-core kernel options
 CASE_FORMS = {"tc_pair": {"tc_pair": True}, "tc_one": {"tc_one": True}, "tc_fp32": {"tc_no16": True},
               "tc_pair_fp32": {"tc_pair": True, "tc_no16": True}}
+# tc_kernel name -> (search kernel, states per accumulator)
+TC_KERNEL_NAMES = {"pair_u16": ("tc_pair_kernel", 2), "pair": ("tc_pair_kernel", 2)}
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
 
@@ -369,8 +371,9 @@ def batch_measure(steps: int, warmup: int, with_baselines: bool) -> dict:
     by CUDA events around the graph launch (max of nothing: one GPU); e2e = wall time of the
     public call with host-resident matrices (packing, H2D, the graph, D2H, decoding).  The
     roofline fraction covers the tensor-core pass-1 kernels of the launch-by-launch run (the
-    instances with n >= 24; 32 flop per state), against the measured bf16 peak and against the
-    int8 dense peak (twice the bf16 figure, the B200's nominal ratio)."""
+    instances with n >= 24; 32 flop per state, of which the batched 16-bit pair kernel runs half
+    on the tensor pipe), against the measured bf16 peak and against the int8 dense peak (twice
+    the bf16 figure, the B200's nominal ratio)."""
     import torch
     import qubo_b200  # noqa: F401
     from qubo_b200 import _lib, configs
@@ -401,9 +404,12 @@ def batch_measure(steps: int, warmup: int, with_baselines: bool) -> dict:
     peak, _, peak_kind = _peaks()
     kms = statistics.median(k_ms)
     tflops = tc_states * FLOPS_PER_STATE_TC / (kms * 1e-3) / 1e12
+    tck = next((r["plan"]["tc_kernel"] for r in res if r["form"] == "tc"), None)
+    per_acc = TC_KERNEL_NAMES.get(tck or "", ("tc_pass1_kernel", 1))[1]
     out = {"metric": "states/s (4096-instance batch, exact FP64 argmin each)", "value": states / (ms * 1e-3),
            "unit": "states/s", "steps": steps, "warmup": max(3, warmup), "ms_per_step": ms,
-           "dtype": "f32 (f16 digit operands, fp32 accumulate; FP64 re-scoring)",
+           "dtype": ("f32 accumulate of f16 integer digits (values rounded to a power-of-two unit, 16-bit minima); "
+                     "FP64 re-scoring") if tck == "pair_u16" else "f32 (f16 digit operands, fp32 accumulate; FP64 re-scoring)",
            "config": {"workload": BATCH_WORKLOAD, "states_per_step": states, "instances": len(Qs),
                       "launch": "one CUDA graph (uploads, six kernels, result copy)",
                       "l2": "flushed between steps (256 MiB write)"},
@@ -413,7 +419,8 @@ def batch_measure(steps: int, warmup: int, with_baselines: bool) -> dict:
            "launch_by_launch": {"ms_per_step": statistics.median(p_ms), "value": states / (statistics.median(p_ms) * 1e-3)},
            "roofline": {"bound": "tensor", "kernel": "pass-1 kernels (tensor-core items n >= 24, Gray items below)",
                         "kernel_ms": kms, "achieved": tflops, "unit": "TFLOP/s", "tc_states": tc_states,
-                        "flops_per_state": FLOPS_PER_STATE_TC,
+                        "flops_per_state": FLOPS_PER_STATE_TC, "tc_kernel": tck,
+                        "tensor_flops_per_state": FLOPS_PER_STATE_TC // per_acc,
                         "frac_bf16": tflops / peak, "peak_bf16": peak, "peak_bf16_kind": f"bf16 dense burst, {peak_kind}",
                         "frac_int8": tflops / (2 * peak), "peak_int8": 2 * peak,
                         "peak_int8_kind": "2 x the bf16 figure (nominal dense int8 : bf16 ratio)"}}
