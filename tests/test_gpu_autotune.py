@@ -49,7 +49,7 @@ def test_autotune_choice_is_used(cuda_ok, n, dtype):
             res = h.solve_batch(Qs)
             for Qb, rb in zip(Qs, res):
                 _check(Qb, rb)
-            drop = lambda p: {k: v for k, v in p.items() if k != "tc_kernel"}  # noqa: E731 (batch: fp32 minima)
+            drop = lambda p: {k: v for k, v in p.items() if k != "tc_kernel"}  # noqa: E731 (the batch's own kernel choice)
             assert res[0]["form"] == form and drop(res[0]["plan"]) == drop(r["plan"])
     finally:
         h.close()
