@@ -136,7 +136,7 @@ def test_sizes_outside_the_scratch_are_rejected(torch_cuda):
 
 def _status(torch, Q, is_integer):
     rc, _, out = _noalloc(torch, Q, is_integer)
-    assert rc == 0  # the problem is queued; its verdict is in the device result
+    assert rc == 0  # the problem is queued; its status is in the device result
     return _read(torch, out)
 
 
