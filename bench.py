@@ -35,7 +35,7 @@ TC_VARIANTS = {"u16": {"tc_one": True}, "fp32": {"tc_no16": True}, "pair": {"tc_
 CASE_FORMS = {"tc_pair": {"tc_pair": True}, "tc_one": {"tc_one": True}, "tc_fp32": {"tc_no16": True},
               "tc_pair_fp32": {"tc_pair": True, "tc_no16": True}}
 # tc_kernel name -> (search kernel, states per accumulator)
-TC_KERNEL_NAMES = {"pair_u16": ("tc_pair_kernel", 2), "pair": ("tc_pair_kernel", 2)}
+TC_KERNEL_NAMES = {"pair_u16": ("tc_pair_kernel", 2), "pair": ("tc_pair_fp32_kernel", 2)}
 N_VARS = 36
 WORKLOAD = "6-city TSP as QUBO, 36 variables, integer distances U{1..100} (seed 0), int32 Q"
 

@@ -1245,7 +1245,6 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
       float gamma[8];
       for (int b = 0; b < 8; ++b) gamma[b] = (float)(W[(size_t)(n - 16) * n + (n - 1 - b)] * sg[k]);
       qb::tc2_u16_tables(gamma, dm, &tc_tabs[k]);
-      tc_tabs[k].dmin = dm;
     }
     if (tc_pair) {
       for (size_t k = 0; k < tcs.size(); ++k) {
@@ -1378,7 +1377,7 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     const qb::TcSmemLayout L = qb::tc_layout(n_tc_max);
     if (tc_pair) {  // plus the second tile's row terms of each B stage
       sm_tc = std::max<size_t>(L.total + qb::kTcBStages * 128 * 4, 120 * 1024) + 1024;
-      QB_CUDA(cudaFuncSetAttribute(qb::tc_pair_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
+      QB_CUDA(cudaFuncSetAttribute(qb::tc_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
     } else {
       sm_tc = std::max<size_t>(L.total, 120 * 1024) + 1024;
       QB_CUDA(cudaFuncSetAttribute(qb::tc_pass1_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tc));
@@ -1413,10 +1412,12 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
     if (!tcs.empty()) {
       QB_CUDA(cudaMemcpyAsync(B[10].p, Wtc, wtc_used * sizeof(double), cudaMemcpyHostToDevice, st));
       QB_CUDA(cudaMemsetAsync(tc_err, 0, 16, st));
-      if (tc_pair)
-        qb::tc_pair_items_kernel<<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(
-            P, static_cast<const qb::Tc2Tab*>(B[14].p));
-      else
+      if (tc_pair) {
+        qb::Tc2Params Q2{};
+        Q2.P = P;
+        Q2.tabs = static_cast<const qb::Tc2Tab*>(B[14].p);
+        qb::tc_pair_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(Q2);
+      } else
         qb::tc_pass1_kernel<true><<<(unsigned)(first.size() - 1), qb::kTcThreads, sm_tc, st>>>(P);
       ++h->kernels;
     }

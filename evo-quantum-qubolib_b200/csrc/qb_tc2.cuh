@@ -23,11 +23,12 @@
 // 2^gl tiles (2^(gl-1) pairs, gl >= 5) 8 records, as in qb_tc.cuh (kGeomTC); a pair never
 // straddles two blocks.
 //
-// fp32 pair form (kU16 = false): the partner's values by one fma per state (gamma of the 5
+// fp32 pair form (tc_pair_fp32_kernel): the partner's values by one fma per state (gamma of the 5
 // low u bits as constant operands, the 3 high u bits added to each 32-column chunk's minimum)
 // and 3-input fp32 minima.
 //
-// 16-bit pair form (kU16, tc2_u16_eligible).  As in the one-state 16-bit epilogue (qb_tc.cuh,
+// 16-bit pair form (tc_pair_kernel<kItems>: one problem, or the batch's work items;
+// tc2_u16_eligible, tc2_u16_quantized).  As in the one-state 16-bit epilogue (qb_tc.cuh,
 // tc_u16_eligible) the accumulator is an integer in [2^23, 2^24) whose fp32 pattern holds a
 // 16-bit value in its low half, loaded two columns per register (.pack::16b).  Here the MMA
 // computes F = D~ + 2^23 - Dlow_s with D~(y, u) = D(y, u) + s * X(u), X the gamma of the chunk
@@ -68,15 +69,22 @@ namespace qb {
 // per-state error bound of the float-digit pair form (unscaled units)
 inline double tc2_error_bound(double abs_sum) { return 264.0 * abs_sum * 5.9604644775390625e-08 + 1e-300; }
 
+// the 16-bit pair form's constants of one problem (one sign per accumulator stage: [0] for
+// s = +1, [1] for s = -1), in the problem's units
+struct Tc2Tab {
+  float gx[3];               // gamma of the chunk bits u4, u5, u6
+  float k0s[2];              // 2^23 - Dlow_s, the offset of the column term
+  float dmin;                // lower bound of every accumulator value D
+  uint32_t corr_t[2][8];     // tile t: correction of chunk c (u4 = c & 1, u5, u6 = c >> 1), both halves
+  uint32_t corr_p[2][2][8];  // partner: correction of position k (u1..u3) in column half hh (u7)
+};
+
 struct Tc2Params {
   TcParams P;       // n, nt, gl, stall, exact, inv_scale, W, tile_begin, groups, groups_per_cta, rec, err
-  alignas(8) float g5[32];     // gamma of register k of a 32-column chunk: sum_{j < 5} w_j k_j (scaled W)
-  float whi[3];     // w_5, w_6, w_7: gamma of u bits 5..7 (scaled W)
-  // 16-bit form (one sign per accumulator stage: [0] for s = +1, [1] for s = -1)
-  float gx[3];             // gamma of the chunk bits u4, u5, u6
-  float k0s[2];            // 2^23 - Dlow_s, the offset of the column term
-  uint32_t corr_t[2][8];   // tile t: correction of chunk c (u4 = c & 1, u5, u6 = c >> 1), both halves
-  uint32_t corr_p[2][2][8];  // partner: correction of position k (u1..u3) in column half hh (u7)
+  alignas(8) float g5[32];     // fp32 form: gamma of register k of a 32-column chunk, sum_{j < 5} w_j k_j
+  float whi[3];     // fp32 form: w_5, w_6, w_7, the gamma of u bits 5..7 (scaled W)
+  Tc2Tab tab;       // 16-bit form, one problem (tc_pair_kernel<false>)
+  const Tc2Tab* tabs;  // 16-bit form, work items: per item (tc_pair_kernel<true>)
 };
 
 // u bits that form the 16-bit pair epilogue's chunks (their gamma is folded into the MMA)
@@ -143,20 +151,11 @@ inline bool tc2_u16_quantized(int n, const double* W, double abs_sum, double* si
   return true;
 }
 
-// per-item constants of the batched 16-bit pair kernel (tc_pair_items_kernel): those of
-// Tc2Params for the item's problem, and its Dmin
-struct Tc2Tab {
-  float gx[3];
-  float k0s[2];
-  float dmin;
-  uint32_t corr_t[2][8];
-  uint32_t corr_p[2][2][8];
-};
 
-// the 16-bit pair form's constant tables from gamma (integers in the kernel's units, rounded
-// here) and Dmin, into Tc2Params or Tc2Tab
-template <class Tab>
-inline void tc2_u16_tables(const float* gamma, float dmin, Tab* Q) {
+// the 16-bit pair form's constants from gamma (integers in the kernel's units, rounded here)
+// and Dmin
+inline void tc2_u16_tables(const float* gamma, float dmin, Tc2Tab* Q) {
+  Q->dmin = dmin;
   int64_t g[8];
   for (int j = 0; j < 8; ++j) g[j] = (int64_t)std::llrint(gamma[j]);
   for (int b = 0; b < 3; ++b) Q->gx[b] = (float)g[kTc2ChunkBits[b]];
@@ -229,8 +228,7 @@ __device__ __forceinline__ uint32_t umin8(uint32_t a, uint32_t b, uint32_t c, ui
   return __vimin3_u16x2(__vimin3_u16x2(a, b, c), __vimin3_u16x2(d, e, f), umin2(g, h));
 }
 
-template <bool kU16>
-__global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_constant__ Tc2Params Q) {
+__global__ void __launch_bounds__(kTcThreads, 1) tc_pair_fp32_kernel(const __grid_constant__ Tc2Params Q) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   const TcParams& P = Q.P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -290,42 +288,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
   for (int e = tid; e < 128 * 16; e += kTcThreads) {
     int y = e >> 4, k = e & 15;
     float v;
-    if (kU16)  // A[y][i] = y_i (i < 7); digit weights: T (slots 8, 9) 1, 2048; constant (10-12) 1, 2048, 32768
-      v = k < 7 ? (float)((y >> k) & 1)
-                : (k == 8 || k == 10 ? 1.0f : (k == 9 || k == 11 ? 2048.0f : (k == 12 ? 32768.0f : 0.0f)));
-    else if (k < 14)
+    if (k < 14)
       v = ((y >> (k >> 1)) & 1) ? ((k & 1) ? s1 : 1.0f) : 0.0f;
     else
       v = (k & 1) ? s1 : 1.0f;
     *reinterpret_cast<__half*>(Asm + kmaj_off(y, k)) = __float2half_rn(v);
   }
   // B operand, coupling columns (same in every stage)
-  if (kU16) {
-    // one exact fp16 value per coupling row (|(V u)_i| <= 2048), zeros in the unused K slots
-    for (int e = tid; e < kTcN * 16; e += kTcThreads) {
-      const int u = e >> 4, k = e & 15;
-      if (k >= 8 && k < 13) continue;  // T's digits (per pair) and the constant digits (below)
-      double v = 0.0;
-      if (k < 7) {
-        const double* row = Ws + (n - 9 - k) * n;
-        for (int j = 0; j < 8; ++j)
-          if ((u >> j) & 1) v += row[n - 1 - j];
-      }
-      // an integer in the kernel's units (rint: the identity on the exact path)
-      const __half hv = __float2half_rn((float)rint(v));
-      for (int s = 0; s < kTcBStages; ++s) *reinterpret_cast<__half*>(Bsm + s * kTcN * 32 + kmaj_off(u, k)) = hv;
-    }
-  } else {
-    for (int e = tid; e < kTcN * 7; e += kTcThreads) {
-      int u = e / 7, i = e % 7;
-      const double* row = Ws + (n - 9 - i) * n;
-      double v = 0.0;
-      for (int j = 0; j < 8; ++j)
-        if ((u >> j) & 1) v += row[n - 1 - j];
-      __half2 dg = digits((float)v, exact);
-      for (int s = 0; s < kTcBStages; ++s)
-        *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
-    }
+  for (int e = tid; e < kTcN * 7; e += kTcThreads) {
+    int u = e / 7, i = e % 7;
+    const double* row = Ws + (n - 9 - i) * n;
+    double v = 0.0;
+    for (int j = 0; j < 8; ++j)
+      if ((u >> j) & 1) v += row[n - 1 - j];
+    __half2 dg = digits((float)v, exact);
+    for (int s = 0; s < kTcBStages; ++s)
+      *reinterpret_cast<__half2*>(Bsm + s * kTcN * 32 + kmaj_off(u, 2 * i)) = dg;
   }
   for (int u = tid; u < kTcN; u += kTcThreads) {
     double e = 0.0;
@@ -337,22 +315,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
         if ((u >> j2) & 1) e += row[n - 1 - j2];
     }
     EU[u] = (float)e;
-    if (kU16) {
-      // the column term's constant part E_U(u) + s X(u) + 2^23 - Dlow_s in three exact digits;
-      // B stage bs always holds pairs of parity bs & 1, hence one sign
-      const double x = ((u >> 4) & 1 ? (double)Q.gx[0] : 0.0) + ((u >> 5) & 1 ? (double)Q.gx[1] : 0.0) +
-                       ((u >> 6) & 1 ? (double)Q.gx[2] : 0.0);
-      for (int bs = 0; bs < kTcBStages; ++bs) {
-        const uint32_t neg = (uint32_t)(((i_begin >> 1) + (uint64_t)bs) & 1ull);
-        const double c = rint(e) + (neg ? -x : x) + (double)Q.k0s[neg];
-        const double d2 = floor(c * (1.0 / 32768.0)), rem = c - 32768.0 * d2;
-        const double d1 = floor(rem * (1.0 / 2048.0)), d0 = rem - 2048.0 * d1;
-        unsigned char* Bst = Bsm + bs * kTcN * 32;
-        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 10)) = __float2half_rn((float)d0);
-        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 11)) = __float2half_rn((float)d1);
-        *reinterpret_cast<__half*>(Bst + kmaj_off(u, 12)) = __float2half_rn((float)d2);
-      }
-    }
   }
   for (int y = tid; y < 128; y += kTcThreads) {
     double e = 0.0;
@@ -505,16 +467,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
           if (r & 1) cr += f5;
           if (r & 2) cr += f6;
           if (r & 4) cr += f7;
-          if (kU16) {
-            // the tile-dependent part T(u) = (t^T W_TU) u of the column term, rounded to an
-            // integer in the kernel's units (the identity on the exact path), |T| < 2^22: digits
-            // d0 in [0, 2048) and d1 = floor(T / 2048), both exact in fp16
-            const float tq = rintf(cr);
-            const float d1 = floorf(tq * (1.0f / 2048.0f));
-            dg[r] = __floats2half2_rn(fmaf(-2048.0f, d1, tq), d1);
-          } else {
-            dg[r] = digits(EU[lane + 32 * r] + cr, exact);
-          }
+          dg[r] = digits(EU[lane + 32 * r] + cr, exact);
         }
       }
 #pragma unroll
@@ -535,13 +488,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
       ok = mbar_wait(&b_empty[bs], ((p >> 3) & 1u) ^ 1u, abort_flag);
       if (!ok) break;
       unsigned char* Bst = Bsm + bs * kTcN * 32;
-      if (kU16) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 8)) = dg[r];
-      } else {
-#pragma unroll
-        for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
-      }
+      for (int r = 0; r < 8; ++r) *reinterpret_cast<__half2*>(Bst + kmaj_off(lane + 32 * r, 14)) = dg[r];
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         Rs[bs * 128 + lane + 32 * r] = ra[r];
@@ -562,142 +510,57 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
     const int y = q * 32 + lane;
     const float inf = __int_as_float(0x7f800000);
     float rmin = inf;
-    if (kU16) {
-      const uint32_t sp = (uint32_t)cq >> 1;  // pair parity = accumulator stage
-      const uint32_t hh = (uint32_t)cq & 1u;  // column half: u bit 7
-      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
-      // every pair of this warp has parity sp, so one sign: s = -1 when tile 2p has t bit 0 set
-      const uint32_t neg = (uint32_t)(((i_begin >> 1) + sp) & 1ull);
-      uint32_t ct[8], cp[8];  // corrections per chunk (tile 2p) and per position (tile 2p + 1)
+    const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
+    const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
+    const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
+    // gamma of u bits 5..7 for the four 32-column chunks of this half
+    float ghi[4];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        ct[c] = Q.corr_t[neg][c];
-        cp[c] = Q.corr_p[neg][hh][c];
-      }
-      // the row terms biased by -2^23: a packed minimum m becomes the float 2^23 + m by
-      // placing its 16 bits under the exponent pattern 0x4B00 (exact for m < 2^16)
-      const float rbias = P.dmin - 8388608.0f;
-      // one pair: wait for its accumulator stage, load it, release it and fold both tiles'
-      // minima into rmin; false when the wait ran out
-      auto pair_step = [&](uint32_t p) -> bool {
-        const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-        // acc_full completes after the MMA thread saw this pair's B stage full: the row terms
-        // written with the stage are visible once it has
-        if (!mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag)) return false;
-        tc_fence_after();
-        // the warp's 128 columns at once, two per register; released before the minima.
-        // Register j of load L holds u = 128 hh + 32 L + 2 j + (0 | 1): chunk c = 2 L + (j >> 3)
-        // (u bits 4, 5, 6), position k = j & 7 (u bits 1, 2, 3)
-        uint32_t r[4][16];
-        QB_TC_LD16P(tbase, r[0]);
-        QB_TC_LD16P(tbase + 32, r[1]);
-        QB_TC_LD16P(tbase + 64, r[2]);
-        QB_TC_LD16P(tbase + 96, r[3]);
-        const float R1 = Rs[bs * 128 + y] + rbias;
-        const float R2 = Rs2[bs * 128 + y] + rbias;
-        tc_wait_ld();
-#pragma unroll
-        for (int c = 0; c < 4; ++c) reg_fence16(r[c]);
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[sp]);
-        // tile 2p: minimum over each chunk, corrected per chunk; tile 2p + 1: minimum over the
-        // chunks at each position, corrected per position (mod 2^16, exact: every corrected
-        // value is D - Dmin of a state, in [0, 2^16))
-        uint32_t v1[8], v2[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const uint32_t* a = &r[c >> 1][(c & 1) * 8];
-          v1[c] = uadd2(umin8(a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]), ct[c]);
+    for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
+    // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
+    uint32_t rec_left = 1u << (gl - 2);
+    uint32_t Jrec = 0;
+    for (uint32_t p = sp; p < npairs && ok; p += 2) {
+      const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
+      // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
+      const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
+      // acc_full completes after the MMA thread saw this pair's B stage full
+      ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
+      if (!ok) break;
+      const float R1 = Rs[bs * 128 + y];
+      const float R2 = Rs2[bs * 128 + y];
+      tc_fence_after();
+      uint32_t ra[32], rb[32];
+      QB_TC_LD32(tbase, ra);
+      QB_TC_LD32(tbase + 32, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      float m1 = fminf(min32(ra), min32(rb));
+      float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
+      QB_TC_LD32(tbase + 64, ra);
+      QB_TC_LD32(tbase + 96, rb);
+      tc_wait_ld();
+      reg_fence32(ra);
+      reg_fence32(rb);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[sp]);
+      m1 = fminf(m1, fminf(min32(ra), min32(rb)));
+      m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
+      rmin = fmin3(rmin, m1 + R1, m2 + R2);
+      if (--rec_left == 0) {
+        const float wm = warp_min_f(rmin) * P.inv_scale;
+        if (lane == 0) {
+          float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
+          if (wm >= 0.f)
+            atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
+          else
+            atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
         }
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-          v2[k] = uadd2(umin8(r[0][k], r[0][k + 8], r[1][k], r[1][k + 8], r[2][k], r[2][k + 8], r[3][k], r[3][k + 8]),
-                        cp[k]);
-        const uint32_t m1 = umin8(v1[0], v1[1], v1[2], v1[3], v1[4], v1[5], v1[6], v1[7]);
-        const uint32_t m2 = umin8(v2[0], v2[1], v2[2], v2[3], v2[4], v2[5], v2[6], v2[7]);
-        const float a1 = fminf(__uint_as_float(__byte_perm(m1, 0x4B000000u, 0x7610)),
-                               __uint_as_float(__byte_perm(m1, 0x4B000000u, 0x7632)));
-        const float a2 = fminf(__uint_as_float(__byte_perm(m2, 0x4B000000u, 0x7610)),
-                               __uint_as_float(__byte_perm(m2, 0x4B000000u, 0x7632)));
-        rmin = fmin3(rmin, a1 + R1, a2 + R2);
-        return true;
-      };
-      // two of the warp's pairs (p and p + 2) per iteration; every warp has a multiple of 8
-      // pairs and at least 8 per record block (measured: 2.40 -> 2.35 ms at n = 36)
-      uint32_t rec_left = 1u << (gl - 2);
-      uint32_t Jrec = 0;
-      for (uint32_t p = sp; p < npairs && ok; p += 4) {
-        ok = pair_step(p) && pair_step(p + 2);
-        if (!ok) break;
-        rec_left -= 2;
-        if (rec_left == 0) {
-          const float wm = warp_min_f(rmin) * P.inv_scale;
-          if (lane == 0) {
-            float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
-            if (wm >= 0.f)
-              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
-            else
-              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
-          }
-          ++Jrec;
-          rec_left = 1u << (gl - 2);
-          rmin = inf;
-        }
-      }
-    } else {
-      const uint32_t sp = (uint32_t)cq >> 1;   // pair parity = accumulator stage
-      const uint32_t hh = (uint32_t)cq & 1u;   // column half: u bit 7
-      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + sp * (uint32_t)kTcN + hh * 128u;
-      // gamma of u bits 5..7 for the four 32-column chunks of this half
-      float ghi[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) ghi[c] = ((c & 1) ? Q.whi[0] : 0.f) + ((c & 2) ? Q.whi[1] : 0.f) + (hh ? Q.whi[2] : 0.f);
-      // records every 2^gl tiles = 2^(gl-1) pairs, 2^(gl-2) of this warp's parity
-      uint32_t rec_left = 1u << (gl - 2);
-      uint32_t Jrec = 0;
-      for (uint32_t p = sp; p < npairs && ok; p += 2) {
-        const uint32_t bs = p & (uint32_t)(kTcBStages - 1);
-        // s = +1 when tile 2p has t bit 0 clear (its partner sets the bit); i_begin is even
-        const float s = (((i_begin >> 1) + p) & 1ull) ? -1.0f : 1.0f;
-        // acc_full completes after the MMA thread saw this pair's B stage full
-        ok = mbar_wait(&acc_full[sp], (p >> 1) & 1u, abort_flag);
-        if (!ok) break;
-        const float R1 = Rs[bs * 128 + y];
-        const float R2 = Rs2[bs * 128 + y];
-        tc_fence_after();
-        uint32_t ra[32], rb[32];
-        QB_TC_LD32(tbase, ra);
-        QB_TC_LD32(tbase + 32, rb);
-        tc_wait_ld();
-        reg_fence32(ra);
-        reg_fence32(rb);
-        float m1 = fminf(min32(ra), min32(rb));
-        float m2 = fminf(fmaf(ghi[0], s, min32_shift(ra, Q, s)), fmaf(ghi[1], s, min32_shift(rb, Q, s)));
-        QB_TC_LD32(tbase + 64, ra);
-        QB_TC_LD32(tbase + 96, rb);
-        tc_wait_ld();
-        reg_fence32(ra);
-        reg_fence32(rb);
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[sp]);
-        m1 = fminf(m1, fminf(min32(ra), min32(rb)));
-        m2 = fmin3(m2, fmaf(ghi[2], s, min32_shift(ra, Q, s)), fmaf(ghi[3], s, min32_shift(rb, Q, s)));
-        rmin = fmin3(rmin, m1 + R1, m2 + R2);
-        if (--rec_left == 0) {
-          const float wm = warp_min_f(rmin) * P.inv_scale;
-          if (lane == 0) {
-            float* dst = rec + (((uint64_t)Jrec << 3) | ((uint64_t)hh << 2) | (uint64_t)q);
-            if (wm >= 0.f)
-              atomicMin(reinterpret_cast<int*>(dst), __float_as_int(wm));
-            else
-              atomicMax(reinterpret_cast<unsigned*>(dst), __float_as_uint(wm));
-          }
-          ++Jrec;
-          rec_left = 1u << (gl - 2);
-          rmin = inf;
-        }
+        ++Jrec;
+        rec_left = 1u << (gl - 2);
+        rmin = inf;
       }
     }
   }
@@ -713,19 +576,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_con
   }
 }
 
-// The batched 16-bit pair kernel: tc_pair_kernel<true> over a list of work items (runs of
-// record blocks of the batch's problems, qb_batch.cuh), as tc_pass1_kernel<true> does for one
-// state per accumulator.  Every role walks the CTA's tiles in the same order; barrier slots,
-// B stages and phases follow the CTA-wide tile counter jbase (a multiple of 32: every item has
-// a multiple of 2^gl >= 32 tiles), pairs the pair counter jbase / 2.  Between items all roles
-// meet at a CTA barrier with the pipelines empty (the MMA thread waits for its last MMA), so
-// the per-item tables, B operand columns and constants can be rewritten.  tabs[it] holds the
-// 16-bit constants of item it's problem; its W is in the item's units (scaled by sigma).
-__global__ void __launch_bounds__(kTcThreads, 1)
-tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restrict__ tabs) {
+
+// The 16-bit pair form.  kItems = false: one problem, each CTA a contiguous run of its record
+// blocks (one work item), its constants in Q.tab; kItems = true: the CTA's list of work items
+// (runs of record blocks of the batch's problems, qb_batch.cuh), Q.tabs[it] the constants of
+// item it's problem, as tc_pass1_kernel<true> does for one state per accumulator.  Every role
+// walks the CTA's tiles in the same order; barrier slots, B stages and phases follow the
+// CTA-wide tile counter jbase (a multiple of 32: every item has a multiple of 2^gl >= 32
+// tiles), pairs the pair counter jbase / 2.  Between items all roles meet at a CTA barrier
+// with the pipelines empty (the MMA thread waits for its last MMA), so the per-item tables,
+// B operand columns and constants can be rewritten.  W is in the problem's units (scaled by
+// sigma off the exact path).
+template <bool kItems>
+__global__ void __launch_bounds__(kTcThreads, 1) tc_pair_kernel(const __grid_constant__ Tc2Params Q) {
   extern __shared__ __align__(1024) unsigned char tc_smem[];
+  const TcParams& P = Q.P;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const TcSmemLayout L = tc_layout(P.n_max);  // only the W block grows with n
+  const TcSmemLayout L = tc_layout(kItems ? P.n_max : P.n);  // only the W block grows with n
   unsigned char* Asm = tc_smem + L.a_off;
   unsigned char* Bsm = tc_smem + L.b_off;
   uint64_t* bars = reinterpret_cast<uint64_t*>(tc_smem + L.bar_off);
@@ -745,8 +612,20 @@ tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restric
   double* LO = reinterpret_cast<double*>(tc_smem + L.lo_off);
   double* Ws = reinterpret_cast<double*>(tc_smem + L.w_off);
 
-  const uint32_t it_lo = P.item_first[blockIdx.x], it_hi = P.item_first[blockIdx.x + 1];
-  if (it_lo >= it_hi) return;  // uniform per CTA
+  // this CTA's work: one run of record blocks of one problem, or a list of items
+  uint32_t it_lo = 0, it_hi = 1;
+  TcItem one{};
+  if (kItems) {
+    it_lo = P.item_first[blockIdx.x];
+    it_hi = P.item_first[blockIdx.x + 1];
+    if (it_lo >= it_hi) return;  // uniform per CTA
+  } else {
+    const uint64_t g0 = (uint64_t)blockIdx.x * P.groups_per_cta;
+    if (g0 >= P.groups) return;  // uniform per CTA
+    const uint64_t g1 = min(P.groups, g0 + P.groups_per_cta);
+    one = TcItem{P.W, P.rec + (g0 << 3), P.tile_begin + (g0 << P.gl), (g1 - g0) << P.gl, P.n, P.gl, P.exact,
+                 P.inv_scale};
+  }
 
   if (tid == 0) {
     for (int s = 0; s < kTcParamSlots; ++s) {
@@ -780,15 +659,18 @@ tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restric
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  uint32_t jbase = 0;  // CTA-wide tile counter
+  uint32_t jnext = 0;  // CTA-wide tile counter of the next item
   for (uint32_t it = it_lo; it < it_hi; ++it) {
-    const TcItem I = P.items[it];
-    const Tc2Tab& Tb = tabs[it];
+    const TcItem I = kItems ? P.items[it] : one;
+    const Tc2Tab& Tb = kItems ? Q.tabs[it] : Q.tab;
     const int n = I.n, nt = n - 15, gl = I.gl;
     const uint64_t i_begin = I.i_begin, ntiles = I.ntiles;
     float* rec = I.rec;
     const uint64_t t0 = gray64(i_begin);
-    const uint32_t pbase = jbase >> 1;  // CTA-wide pair counter (a multiple of 16)
+    // the CTA-wide tile and pair counters at the item's start (a compile-time 0 for one
+    // problem, so its barrier parities and stages reduce to constants as in a one-item kernel)
+    const uint32_t jbase = kItems ? jnext : 0u;
+    const uint32_t pbase = jbase >> 1;  // a multiple of 16
 
     // ------------------------------------------------------------ per-item set-up
     for (int i = tid; i < n * n; i += kTcThreads) Ws[i] = I.W[i];
@@ -868,7 +750,9 @@ tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restric
     const uint32_t npairs = (uint32_t)(ntiles >> 1);
 
     bool ok = true;
-    if (warp == 0) {
+    if (warp == 0 && P.stall) {
+      // test hook (QB_FLAG_TEST_STALL): nothing is published, every other wait runs out
+    } else if (warp == 0) {
       // ---------------------------------------------------------- tile walk (every tile)
       const int nh = nt - 5;
       double fh[8], gh[7], c[5], eh = 0.0, h0 = 0.0, h1 = 0.0;
@@ -1104,7 +988,7 @@ tc_pair_items_kernel(const __grid_constant__ TcParams P, const Tc2Tab* __restric
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    jbase += (uint32_t)ntiles;
+    jnext = jbase + (uint32_t)ntiles;
     if (*abort_flag) break;  // uniform: read after the barrier
   }
   tc_fence_before();
@@ -1152,11 +1036,11 @@ inline int tc2_launch(const TcPlan& p, const float* gamma, float* rec, void* scr
   Q.whi[2] = gamma[7];
   if (p.u16) {
     P.dmin = p.dmin;
-    tc2_u16_tables(gamma, p.dmin, &Q);
+    tc2_u16_tables(gamma, p.dmin, &Q.tab);
   }
   const TcSmemLayout L = tc_layout(p.n);
   const size_t smem = std::max<size_t>(L.total + kTcBStages * 128 * 4, 120 * 1024) + 1024;
-  auto* kern = p.u16 ? tc_pair_kernel<true> : tc_pair_kernel<false>;
+  auto* kern = p.u16 ? tc_pair_kernel<false> : tc_pair_fp32_kernel;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 4;
   kern<<<(unsigned)ctas, kTcThreads, smem, st>>>(Q);
   ++*kernels;
