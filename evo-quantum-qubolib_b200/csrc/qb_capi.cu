@@ -1241,14 +1241,14 @@ int batch_run(qb_handle* h, const qb_problem* problems, const std::vector<int32_
         tc_pair = false;
         break;
       }
-      if (!(insts[j].exact_digits && ep[k] == 0.0 && sg[k] == 1.0)) insts[j].exact_digits = 0;
       float gamma[8];
       for (int b = 0; b < 8; ++b) gamma[b] = (float)(W[(size_t)(n - 16) * n + (n - 1 - b)] * sg[k]);
       qb::tc2_u16_tables(gamma, dm, &tc_tabs[k]);
     }
-    if (tc_pair) {
+    if (tc_pair) {  // every member fits: only now change the members' plans
       for (size_t k = 0; k < tcs.size(); ++k) {
         qb::BatchInst& I = insts[tcs[k].first];
+        if (ep[k] > 0.0) I.exact_digits = 0;  // rounded values (the digits flag is unused by this kernel)
         I.scale = sg[k];
         I.eps = ep[k];
         I.tc_kernel = 4;

@@ -149,6 +149,26 @@ def test_batch_tensor_core_members_take_the_16bit_pair_kernel(cuda_ok):
         _check(Q, r)
 
 
+def test_batch_falls_back_to_one_state_when_a_member_does_not_fit(cuda_ok):
+    """A tensor-core member the 16-bit pair kernel cannot take (float Q whose u variables have
+    no couplings: a zero value span) keeps the whole batch on the one-state kernel, and every
+    member keeps its own plan: an integer member on exact digits whose values span more than
+    2^16 (which alone would take rounded values) stays exact, a float member keeps its bound."""
+    rng = np.random.default_rng(41)
+    n = 26
+    wide = rng.integers(-2000, 2001, (n, n)).astype(np.int32)
+    Z = rng.standard_normal((n, n))
+    Z[:, n - 8:] = 0.0
+    Z[n - 8:, :] = 0.0
+    F = rng.standard_normal((n, n))
+    Qs = [wide, Z, F]
+    res = _lib.handle(0).solve_batch(Qs)
+    for Q, r in zip(Qs, res):
+        assert r["form"] == "tc" and r["plan"]["tc_kernel"] == "fp32", r["plan"]
+        _check(Q, r)
+    assert res[0]["err_bound"] == 0.0
+
+
 def _same_shapes(Qs, seed):
     """New matrices with the sizes and dtypes of Qs (the same batch shape, other values)."""
     rng = np.random.default_rng(seed)
