@@ -138,6 +138,31 @@ def test_c_abi_host_only_calls():
     assert b"no-allocation" in L.qb_strerror(8)
 
 
+def test_batch_descriptors():
+    """qb_solve_batch's problem descriptors built on the host: sizes, dtype codes and the
+    data address of each matrix (a contiguous copy for a non-contiguous input)."""
+    rng = np.random.default_rng(3)
+    ro = rng.normal(size=(21, 21))
+    ro.flags.writeable = False
+    Qs = [rng.normal(size=(20, 20)).astype(np.float32), ro,
+          rng.integers(-9, 9, size=(24, 24)).astype(np.int16).T,  # non-contiguous
+          np.zeros((0, 0), dtype=np.int32), rng.integers(-9, 9, size=(1, 1)).astype(np.int64)]
+    probs, ns, keep = _lib.Handle._batch_problems(Qs)
+    assert list(ns) == [20, 21, 24, 0, 1]
+    for i, (p, Q) in enumerate(zip(probs, keep)):
+        assert Q.flags.c_contiguous
+        assert p.n == p.ldq == Q.shape[0]
+        assert p.dtype == _lib._DTYPES[Q.dtype]
+        assert (p.q or 0) == Q.__array_interface__["data"][0], i
+        np.testing.assert_array_equal(Q, Qs[i])
+    assert keep[0] is Qs[0] and keep[1] is Qs[1] and keep[2] is not Qs[2]
+    assert len(_lib.Handle._batch_problems([])[0]) == 0
+    with pytest.raises(ValueError):
+        _lib.Handle._batch_problems([np.zeros((2, 3))])
+    with pytest.raises(TypeError):
+        _lib.Handle._batch_problems([np.zeros((2, 2), dtype=np.uint8)])
+
+
 def test_config_generators_match_reference_inputs():
     from qubo_b200 import configs
     cfg = load_golden("configs.json")
