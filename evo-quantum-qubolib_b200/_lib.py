@@ -251,14 +251,12 @@ class Handle:
         count = len(Qs)
         probs, ns, keep = self._batch_problems(Qs)
         o = self.options(**opts)
-        res = (QbResult * count)()
-        rc = load().qb_solve_batch(self._h, probs, count, ctypes.byref(o), res)
+        res = np.zeros(count, dtype=np.dtype(QbResult))  # written in place by the library
+        rc = load().qb_solve_batch(self._h, probs, count, ctypes.byref(o), res.ctypes.data_as(ctypes.POINTER(QbResult)))
         del keep
         if rc:
             _raise(rc, "qb_solve_batch")
-        if not count:
-            return BatchResults(np.zeros(0, dtype=np.dtype(QbResult)), ns)
-        return BatchResults(np.frombuffer(res, dtype=np.dtype(QbResult)).copy(), ns)
+        return BatchResults(res, ns)
 
     def prefix_minima(self, Q: np.ndarray, prefix_bits: int = -1) -> np.ndarray:
         """Per-prefix minimum energies in QBF's Gray visiting order (qb_prefix_minima)."""
