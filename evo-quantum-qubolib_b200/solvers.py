@@ -32,6 +32,7 @@ from __future__ import annotations
 
 import logging
 import multiprocessing as mp
+import os
 import queue as _queue
 import threading
 import time
@@ -59,6 +60,15 @@ def _torch_stream(device: int):
 
 _json_pool = None
 _json_pool_lock = threading.Lock()
+
+
+def _drop_json_pool():  # a forked child has the pool object but not its thread
+    global _json_pool, _json_pool_lock
+    _json_pool = None
+    _json_pool_lock = threading.Lock()
+
+
+os.register_at_fork(after_in_child=_drop_json_pool)
 
 
 def _encode_async(problem, kwargs):

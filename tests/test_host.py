@@ -101,6 +101,28 @@ def test_solution_json_round_trip():
     assert back.N == 5 and back.epochs_cnt == 4
 
 
+def test_solution_json_encoded_on_worker_thread():
+    """The Solution's JSON fields, encoded on a worker thread during the device search, equal
+    the direct encodings; a forked child gets a pool of its own."""
+    from qubo_b200 import _json, solvers
+    prob = Just_Q(np.arange(25, dtype=np.int32).reshape(5, 5))
+    kw = {"device": "cuda:0", "form": "tc", "use_metrics": ["energy_arr"]}
+    pj, ks = solvers._encode_async(prob, kw).result(timeout=30)
+    assert pj == prob.to_json() and ks == _json.encode(kw, indent=4)
+    import warnings
+    with warnings.catch_warnings():  # forking a threaded process is the case under test
+        warnings.simplefilter("ignore", DeprecationWarning)
+        pid = os.fork()
+    if pid == 0:  # child: no thread behind the inherited pool object
+        try:
+            ok = solvers._encode_async(prob, kw).result(timeout=10)[0] == pj
+        except BaseException:  # noqa: BLE001
+            ok = False
+        os._exit(0 if ok else 1)
+    _, status = os.waitpid(pid, 0)
+    assert os.WIFEXITED(status) and os.WEXITSTATUS(status) == 0
+
+
 def test_boundary_errors_without_gpu():
     with pytest.raises(ValueError):
         QBF().solve(Just_Q(np.eye(4, dtype=np.int32)), device="cpu")
