@@ -62,6 +62,29 @@ def test_batch_twice_and_matches_single_calls(cuda_ok):
         assert abs(ra["best_E"] - rs["best_E"]) <= 1e-9 * max(1.0, abs(rs["best_E"]))
 
 
+def test_batch_read_only_and_strided_matrices(cuda_ok):
+    """Members passed as read-only arrays and as non-contiguous views (the descriptors then
+    point at a contiguous copy or come from the array interface) give the answers of their
+    writable contiguous copies and of the oracle."""
+    Qs = _mixed(11, 24)
+    given = []
+    for i, Q in enumerate(Qs):
+        if i % 3 == 0:
+            R = Q.copy()
+            R.flags.writeable = False
+            given.append(R)
+        elif i % 3 == 1:
+            given.append(np.asfortranarray(Q).T.T)  # same values, Fortran order
+        else:
+            given.append(np.ascontiguousarray(Q.T).T)  # a transposed view of Q's transpose
+    h = _lib.handle(0)
+    a = h.solve_batch(given)
+    b = h.solve_batch(Qs)
+    for Q, ra, rb in zip(Qs, a, b):
+        assert (ra["best_X_int"], ra["best_E"]) == (rb["best_X_int"], rb["best_E"])
+        _check(Q, ra)
+
+
 def test_batch_ties_follow_the_split(cuda_ok):
     rng = np.random.default_rng(8)
     Qs = [rng.integers(-2, 3, (n, n)).astype(np.int32) for n in (12, 18, 22, 25)]

@@ -132,6 +132,24 @@ def test_qb_f1_order(cuda_ok, n, seed):
     assert sol.solver_class == "QB_F1" and sol.epochs_cnt == 1 and isinstance(sol.best_E, int)
 
 
+def test_solution_json_fields(cuda_ok):
+    """QBF and QB_F1 solutions carry the problem's and the kwargs' JSON (encoded while the
+    device search runs), equal to the direct encodings; the solution round-trips."""
+    from qubo_b200 import _json
+    from qubo_b200.solution import Solution
+    rng = np.random.default_rng(12)
+    U = rng.integers(-5, 6, (22, 22)).astype(np.int16)
+    prob = Just_Q((np.triu(U) + np.triu(U, 1).T).astype(np.int16))
+    for solver, kw in ((QBF(), {"device": "cuda", "A": 3}), (QB_F1(), {"device": "cuda"})):
+        sol = solver.solve(prob, **kw)
+        assert sol.problem_instance_json == prob.to_json()
+        assert sol.solver_params_json == _json.encode(kw, indent=4)
+        back = Solution.init_from_json(sol.to_json())
+        assert float(back.best_E) == float(sol.best_E)
+    for _ in range(20):  # back-to-back solves reuse the worker thread
+        assert QBF().solve(prob, device="cuda").problem_instance_json == prob.to_json()
+
+
 def test_qb_f1_rejects_non_int16(cuda_ok):
     with pytest.raises(TypeError):
         QB_F1().solve(Just_Q(np.zeros((20, 20), np.int32)), device="cuda")
