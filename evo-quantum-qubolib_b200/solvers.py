@@ -71,16 +71,18 @@ def _drop_json_pool():  # a forked child has the pool object but not its thread
 os.register_at_fork(after_in_child=_drop_json_pool)
 
 
-def _encode_async(problem, kwargs):
-    """A future of (problem.to_json(), the kwargs' JSON): the encoding runs on a worker thread
-    while the library call, which releases the GIL, waits for the device (about 0.1 ms of
-    host work per solve for a 36-variable problem)."""
+def _encode_async(problem, kwargs, Q=None):
+    """A future of the Solution fields that depend on the problem alone: (problem.to_json(),
+    the kwargs' JSON, the Ising offset of Q or None without Q).  They are computed on a worker
+    thread while the library call, which releases the GIL, waits for the device (about 0.1 ms
+    of host work per solve for a 36-variable problem)."""
     global _json_pool
     with _json_pool_lock:
         if _json_pool is None:
             from concurrent.futures import ThreadPoolExecutor
             _json_pool = ThreadPoolExecutor(max_workers=1, thread_name_prefix="qubo_b200-json")
-    return _json_pool.submit(lambda: (problem.to_json(), _json.encode(kwargs, indent=4)))
+    return _json_pool.submit(lambda: (problem.to_json(), _json.encode(kwargs, indent=4),
+                                      None if Q is None else problem.get_Q_Ising_offset(np, Q)))
 
 
 def _check_obsolete(kwargs):
@@ -157,12 +159,12 @@ class QBF(SolverABC):
         if self.A < 0 or self.B < 1 or self.A + self.B != self.N:
             raise ValueError(f"invalid split A={self.A}, B={self.B} for N={self.N}")
         form = kwargs.get("form", "auto")
-        enc = _encode_async(problem, kwargs)  # submitted last: it runs during the device search
+        enc = _encode_async(problem, kwargs, Q)  # submitted last: it runs during the device search
         res = _lib.handle(dev).solve(Q, form=form, tie_rule="qbf", fixed_bits=0, prefix_bits=self.A,
                                      stream=stream)
         self.timer.pick_time("search")
-        problem_json, self.json_str = enc.result()
-        return self._pack(problem, res, kwargs, problem_json)
+        problem_json, self.json_str, offset = enc.result()
+        return self._pack(problem, res, kwargs, problem_json, offset)
 
     def solve_batch(self, problems, **kwargs) -> list:
         """Solve many independent problems in one batched GPU search (qb_solve_batch) and
@@ -193,7 +195,7 @@ class QBF(SolverABC):
             out.append(self._pack(problem, res, kwargs))
         return out
 
-    def _pack(self, problem, res, kwargs, problem_json=None) -> Solution:
+    def _pack(self, problem, res, kwargs, problem_json=None, ising_offset=None) -> Solution:
         best_X = res["best_X"]
         if problem_json is None:
             problem_json = problem.to_json()
@@ -215,7 +217,7 @@ class QBF(SolverABC):
         sol.solver_class = "QBF"
         sol.best_E = self.glob_E
         sol.best_X = best_X
-        sol.ising_offset = problem.get_Q_Ising_offset(np, self.Q)
+        sol.ising_offset = problem.get_Q_Ising_offset(np, self.Q) if ising_offset is None else ising_offset
         if hasattr(problem, "prefix_E"):
             sol.prefix_E = problem.prefix_E
         sol.time_to_solve_ms = self.timer.get_time_from_start()
@@ -260,11 +262,11 @@ class QB_F1(SolverABC):
         self.Q = Q
         self.timer.pick_time("build_Q")
         wrap = bool(kwargs.get("int16_wrap", False))
-        enc = _encode_async(problem, kwargs)  # submitted last: it runs during the device search
+        enc = _encode_async(problem, kwargs, Q)  # submitted last: it runs during the device search
         res = _lib.handle(dev).solve(Q, form=kwargs.get("form", "auto"), tie_rule="qb_f1", fixed_bits=0,
                                      stream=stream, int16_wrap=wrap)
         self.timer.pick_time("Kernel run time")
-        problem_json, self.json_str = enc.result()
+        problem_json, self.json_str, offset = enc.result()
         best_X = res["best_X"]
         sol = Solution(self.N, 1, 1, problem_json, self.json_str)
         sol.state_vectors = StateVectors(wide_vector_matrix=best_X.reshape(1, -1))
@@ -275,7 +277,7 @@ class QB_F1(SolverABC):
         sol.best_X = best_X
         if hasattr(problem, "prefix_E"):
             sol.prefix_E = problem.prefix_E
-        sol.ising_offset = problem.get_Q_Ising_offset(np, Q)
+        sol.ising_offset = offset
         sol.timer = [(t, lbl) for t, lbl in self.timer.times if lbl != "epoch"]
         sol.time_to_solve_ms = self.timer.get_time_from_start()
         sol.search = {k: res[k] for k in ("form", "states", "candidate_records", "pass1_ms", "pass2_ms", "kernel_ms",

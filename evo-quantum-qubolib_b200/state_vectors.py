@@ -31,6 +31,8 @@ class StateVectors:
     def pack_wide_vectors_to_bitwise(self, wide_vectors: np.ndarray, target_dtype=np.uint8) -> np.ndarray:
         if target_dtype not in self.SUPPORTED_TYPES:
             raise TypeError(f"Unsupported target dtype: {target_dtype}. Supported types: {self.SUPPORTED_TYPES}")
+        if target_dtype is np.uint8:  # the default: numpy's LSB-first byte packing is this layout
+            return np.packbits(np.asarray(wide_vectors) != 0, axis=1, bitorder="little")
         rows, length = wide_vectors.shape
         bits = np.dtype(target_dtype).itemsize * 8
         per_row = (length + bits - 1) // bits

@@ -133,8 +133,9 @@ def test_qb_f1_order(cuda_ok, n, seed):
 
 
 def test_solution_json_fields(cuda_ok):
-    """QBF and QB_F1 solutions carry the problem's and the kwargs' JSON (encoded while the
-    device search runs), equal to the direct encodings; the solution round-trips."""
+    """QBF and QB_F1 solutions carry the problem's and the kwargs' JSON and the Ising offset
+    (computed while the device search runs), equal to the direct computations, and the packed
+    state vector of best_X; the solution round-trips."""
     from qubo_b200 import _json
     from qubo_b200.solution import Solution
     rng = np.random.default_rng(12)
@@ -144,6 +145,8 @@ def test_solution_json_fields(cuda_ok):
         sol = solver.solve(prob, **kw)
         assert sol.problem_instance_json == prob.to_json()
         assert sol.solver_params_json == _json.encode(kw, indent=4)
+        assert sol.ising_offset == prob.get_Q_Ising_offset(np, prob.build_Q_matrix())
+        np.testing.assert_array_equal(sol.state_vectors.get_wide_vectors()[0], sol.best_X)
         back = Solution.init_from_json(sol.to_json())
         assert float(back.best_E) == float(sol.best_E)
     for _ in range(20):  # back-to-back solves reuse the worker thread

@@ -107,8 +107,10 @@ def test_solution_json_encoded_on_worker_thread():
     from qubo_b200 import _json, solvers
     prob = Just_Q(np.arange(25, dtype=np.int32).reshape(5, 5))
     kw = {"device": "cuda:0", "form": "tc", "use_metrics": ["energy_arr"]}
-    pj, ks = solvers._encode_async(prob, kw).result(timeout=30)
-    assert pj == prob.to_json() and ks == _json.encode(kw, indent=4)
+    pj, ks, off = solvers._encode_async(prob, kw).result(timeout=30)
+    assert pj == prob.to_json() and ks == _json.encode(kw, indent=4) and off is None
+    Q = prob.build_Q_matrix()
+    assert solvers._encode_async(prob, kw, Q).result(timeout=30)[2] == prob.get_Q_Ising_offset(np, Q)
     import warnings
     with warnings.catch_warnings():  # forking a threaded process is the case under test
         warnings.simplefilter("ignore", DeprecationWarning)
