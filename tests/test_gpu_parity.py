@@ -389,6 +389,29 @@ def test_tensor_core_pair_16bit_float(cuda_ok, n, seed):
         assert best["best_X_int"] == ref["best_X_int"]
 
 
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_float_near_ties_below_the_error_bound(cuda_ok, seed):
+    """A 5-city TSP QUBO (its optimal tours tie: every tour in both directions) plus symmetric
+    float noise of 1e-6: the optima differ by far less than the pass-1 error bound of the
+    rounded 16-bit pair form, so every record holding one must become a candidate and the
+    FP64 re-walk must pick the oracle's state, in every form."""
+    from qubo_b200.problems import TSP
+    rng = np.random.default_rng(seed)
+    w = rng.integers(1, 101, (5, 5))
+    w = np.triu(w, 1)
+    w = w + w.T
+    noise = rng.standard_normal((25, 25)) * 1e-6
+    Q = TSP.qubo_from_distances(w.astype(np.float64)) + (noise + noise.T) / 2
+    ref = oracle.qbf_port(Q)
+    h = _lib.handle(0)
+    r = h.solve(Q, form="tc")
+    assert r["plan"]["tc_kernel"] == "pair_u16" and r["err_bound"] > 1e-3
+    assert r["candidate_records"] >= 2
+    _check(Q, _as_sol(r), ref)
+    for form in ("gray", "exact", "auto"):
+        _check(Q, _as_sol(h.solve(Q, form=form)), ref)
+
+
 def test_tensor_core_pair_16bit_rounded_integers(cuda_ok):
     """Integer Q beyond the exact-digit range (sum|Q| > 2^22) takes the 16-bit pair form on
     rounded values with a nonzero error bound; pass 2 makes the answer bit-exact.  A problem
