@@ -1,4 +1,5 @@
-// qb_tc2.cuh -- tensor-core form with two states per accumulator (tile pairs), one problem.
+// qb_tc2.cuh -- tensor-core form with two states per accumulator (tile pairs): one problem,
+// or (16-bit form) the work items of a batch.
 //
 // Same decomposition as qb_tc.cuh (t: tile index in Gray order, y: the 128 MMA rows, u: the
 // 256 MMA columns; E(t, y, u) = R_t(y) + C_t(u) + y^T V u), but the Gray-ordered tiles are
@@ -11,7 +12,7 @@
 // partner tile's value from it.  Every TMEM accumulator thus stands for two states, which
 // halves the MMAs, accumulator round trips and TMEM loads per state.  Measured on B200
 // (n = 36 TSP QUBO, 2^36 states): fp32 pair form 3.83 ms, 16-bit pair form (below) 2.36 ms,
-// against 3.93-3.95 ms for one state per accumulator; the 16-bit pair form is the default
+// against 3.8-3.95 ms for one state per accumulator; the 16-bit pair form is the default
 // where it applies, and qb_autotune times both forms.
 //
 // Roles, pipelines, records and bounded waits are those of tc_pass1_kernel<false>
