@@ -1,0 +1,146 @@
+"""Host-side planning of the 16-bit pair form (csrc/qb_tc2.cuh), checked on the CPU.
+
+The kernel reads each accumulator as a 16-bit value v(u) = D(u) + s*X(u) - Dmin - lo_s
+(F = D~ + 2^23 - Dlow_s in fp32, low half of the bit pattern) and adds one packed constant:
+per chunk c = (u4, u5, u6) for tile t, giving D(u) - Dmin, and per position k = (u1, u2, u3),
+half u0 and column half u7 for the partner tile, giving D(u) + s*gamma(u) - Dmin, all modulo
+2^16.  The harness (tests/tc2_tables_harness.cpp) exports the library's own table builder
+and planning functions; this test emulates the kernel's arithmetic with them."""
+import ctypes
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "evo-quantum-qubolib_b200", "csrc")
+CUDA_INC = "/usr/local/cuda/include"
+
+
+class Tc2Tab(ctypes.Structure):
+    _fields_ = [("gx", ctypes.c_float * 3), ("k0s", ctypes.c_float * 2), ("dmin", ctypes.c_float),
+                ("corr_t", (ctypes.c_uint32 * 8) * 2), ("corr_p", ((ctypes.c_uint32 * 8) * 2) * 2)]
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    gxx = shutil.which("g++")
+    if gxx is None or not os.path.isdir(CUDA_INC):
+        pytest.skip("g++ or the CUDA headers are not available")
+    out = str(tmp_path_factory.mktemp("tc2") / "tc2_tables.so")
+    subprocess.run([gxx, "-std=c++17", "-O1", "-fPIC", "-shared", "-I", CSRC, "-I", CUDA_INC,
+                    os.path.join(HERE, "tc2_tables_harness.cpp"), "-o", out], check=True)
+    L = ctypes.CDLL(out)
+    dp, fp = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)
+    L.h_tc2_u16_eligible.argtypes = [ctypes.c_int, dp, fp]
+    L.h_tc2_u16_quantized.argtypes = [ctypes.c_int, dp, ctypes.c_double, dp, fp, dp]
+    L.h_tc2_u16_tables.argtypes = [fp, ctypes.c_float, ctypes.POINTER(Tc2Tab)]
+    assert L.h_tc2_tab_size() == ctypes.sizeof(Tc2Tab)
+    return L
+
+
+def _tables(L, gamma, dmin):
+    g = np.asarray(gamma, dtype=np.float32)
+    t = Tc2Tab()
+    L.h_tc2_u16_tables(g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), float(dmin), ctypes.byref(t))
+    return t
+
+
+def _half(word, d):
+    return (int(word) >> (16 * d)) & 0xFFFF
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_corrections_recover_both_tiles(harness, seed):
+    rng = np.random.default_rng(seed)
+    gamma = rng.integers(-2000, 2001, 8)
+    if seed == 0:
+        gamma[[4, 5, 6]] = [2000, -2000, 0]  # extreme and zero chunk couplings
+    dmin = float(rng.integers(-40000, 1000))
+    t = _tables(harness, gamma, dmin)
+    u = np.arange(256)
+    bit = lambda b: (u >> b) & 1  # noqa: E731
+    X = sum(int(gamma[b]) * bit(b) for b in (4, 5, 6))
+    gam = sum(int(gamma[b]) * bit(b) for b in range(8))
+    c, k, d, hh = (u >> 4) & 7, (u >> 1) & 7, u & 1, u >> 7
+    assert [int(v) for v in t.gx] == [int(gamma[b]) for b in (4, 5, 6)] and t.dmin == dmin
+    margin = int(np.abs(gamma).sum())
+    for neg, s in ((0, 1), (1, -1)):
+        lo = sum(min(0, s * int(gamma[b])) for b in (4, 5, 6))
+        assert t.k0s[neg] == 2.0 ** 23 - (dmin + lo)
+        for trial in range(4):
+            # accumulator values D(u) whose partner values D + s*gamma(u) are values too
+            D = dmin + margin + rng.integers(0, 30000, 256)
+            v = D + s * X - dmin - lo
+            assert v.min() >= 0 and v.max() < 1 << 16  # the 16-bit read is exact
+            for j in range(256):
+                ct = _half(t.corr_t[neg][c[j]], d[j])
+                assert _half(t.corr_t[neg][c[j]], 0) == _half(t.corr_t[neg][c[j]], 1)
+                assert (int(v[j]) + ct) & 0xFFFF == D[j] - dmin
+                cp = _half(t.corr_p[neg][hh[j]][k[j]], d[j])
+                assert (int(v[j]) + cp) & 0xFFFF == D[j] + s * gam[j] - dmin
+
+
+def _upper(rng, n, scale):
+    W = np.triu(rng.standard_normal((n, n)) * scale)
+    return W
+
+
+@pytest.mark.parametrize("n,scale,seed", [(24, 1.0, 0), (30, 37.5, 1), (36, 0.01, 2), (36, 1e4, 3)])
+def test_rounded_unit_is_the_largest_power_of_two_within_limits(harness, n, scale, seed):
+    rng = np.random.default_rng(seed)
+    W = _upper(rng, n, scale)
+    abs_sum = float(np.abs(W).sum())
+    sg, dm, ep = ctypes.c_double(), ctypes.c_float(), ctypes.c_double()
+    dp = ctypes.POINTER(ctypes.c_double)
+    ok = harness.h_tc2_u16_quantized(n, W.ctypes.data_as(dp), abs_sum, ctypes.byref(sg), ctypes.byref(dm),
+                                     ctypes.byref(ep))
+    assert ok == 1
+    sigma = sg.value
+    assert sigma > 0 and np.log2(sigma) == int(np.log2(sigma))  # a power of two
+    # the kernel's limits, restated from the W entries the 16-bit form reads
+    rows = [W[n - 9 - i, n - 8:] for i in range(7)]
+    rowmax = max(max(r[r > 0].sum(), -r[r < 0].sum()) for r in rows)
+    vals = [W[n - 9 - i, n - 1 - j] for i in range(7) for j in range(8)]
+    for j in range(8):
+        a = n - 1 - j
+        vals += [W[a, a]] + [W[a, n - 1 - j2] for j2 in range(j)] + [W[t, a] for t in range(n - 15)]
+    vals = np.array(vals)
+    lo, hi = vals[vals < 0].sum(), vals[vals > 0].sum()
+    gA = sum(abs(W[n - 16, n - 1 - b]) for b in (4, 5, 6))
+
+    def fits(sg):
+        return sg * rowmax <= 2047 and sg * (hi - lo + gA) + 40 <= 65535
+
+    assert fits(sigma) and not fits(2 * sigma) and sigma * (hi - lo) >= 1024
+    assert dm.value == np.floor(sigma * lo) - 12
+    assert ep.value == pytest.approx(10 / sigma + abs_sum * 2.0 ** -16, rel=1e-15)
+
+
+def test_rounded_form_refuses_a_coarse_or_empty_span(harness):
+    dp = ctypes.POINTER(ctypes.c_double)
+    sg, dm, ep = ctypes.c_double(), ctypes.c_float(), ctypes.c_double()
+    n = 26
+    Z = np.zeros((n, n))  # no couplings touch the u variables: zero span
+    assert harness.h_tc2_u16_quantized(n, Z.ctypes.data_as(dp), 0.0, ctypes.byref(sg), ctypes.byref(dm),
+                                       ctypes.byref(ep)) == 0
+    assert harness.h_tc2_u16_quantized(19, Z.ctypes.data_as(dp), 0.0, ctypes.byref(sg), ctypes.byref(dm),
+                                       ctypes.byref(ep)) == 0  # below 20 variables
+
+
+def test_exact_eligibility_needs_room_for_the_chunk_couplings(harness):
+    """Integer W whose value span fits 16 bits but not with the chunk couplings added."""
+    n = 24
+    fp = ctypes.c_float()
+    dp = ctypes.POINTER(ctypes.c_double)
+    W = np.zeros((n, n))
+    W[n - 16, n - 1 - 4] = 100.0  # a chunk coupling of the pair variable
+    assert harness.h_tc2_u16_eligible(n, W.ctypes.data_as(dp), ctypes.byref(fp)) == 1
+    # the value span counts the coupling (100) once; the chunk offset adds |gamma_4| = 100
+    W[n - 1, n - 1] = 65535.0 - 200.0  # span + offset = 2^16 - 1: still exact in 16 bits
+    assert harness.h_tc2_u16_eligible(n, W.ctypes.data_as(dp), ctypes.byref(fp)) == 1
+    assert fp.value == 0.0  # Dmin: no negative couplings
+    W[n - 1, n - 1] = 65535.0 - 199.0  # span + offset = 2^16: refused, though the span fits
+    assert harness.h_tc2_u16_eligible(n, W.ctypes.data_as(dp), ctypes.byref(fp)) == 0
