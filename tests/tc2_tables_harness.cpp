@@ -1,6 +1,7 @@
-// Host-only harness for tests/test_tc2_tables.py: exports the 16-bit pair form's host-side
-// planning (eligibility, the power-of-two unit of the rounded form, the per-problem table of
-// constants) from the library's own header so the test can check their algebra on the CPU.
+// Host-only harness for tests/test_tc2_tables.py: exports the tensor-core forms' host-side
+// planning (the shard plan, the 16-bit pair form's eligibility, the power-of-two unit of its
+// rounded form, its per-problem table of constants) from the library's own headers so the
+// test can check them on the CPU.
 // Built by the test with g++; not part of the library.
 #include "qb_tc2.cuh"
 
@@ -15,5 +16,20 @@ int h_tc2_u16_quantized(int n, const double* W, double abs_sum, double* sigma, f
 }
 
 void h_tc2_u16_tables(const float* gamma, float dmin, qb::Tc2Tab* out) { qb::tc2_u16_tables(gamma, dmin, out); }
+
+// tc_plan of one shard: u64 {tile_begin, tile_end, rec_begin, rec_count, states},
+// f64 {scale, eps}, i32 {nt, gl, exact}
+void h_tc_plan(int n, int is_int, double abs_sum, int shard_idx, int shard_cnt, int gl, uint64_t* u64, double* f64,
+               int* i32) {
+  qb::TcPlan p;
+  qb::tc_plan(n, is_int != 0, abs_sum, shard_idx, shard_cnt, &p, gl);
+  const uint64_t u[5] = {p.tile_begin, p.tile_end, p.rec_begin, p.rec_count, p.states};
+  for (int i = 0; i < 5; ++i) u64[i] = u[i];
+  f64[0] = p.scale;
+  f64[1] = p.eps;
+  i32[0] = p.nt;
+  i32[1] = p.gl;
+  i32[2] = p.exact ? 1 : 0;
+}
 
 }  // extern "C"

@@ -1,4 +1,5 @@
-"""Host-side planning of the 16-bit pair form (csrc/qb_tc2.cuh), checked on the CPU.
+"""Host-side planning of the tensor-core forms (csrc/qb_tc.cuh, csrc/qb_tc2.cuh), checked on
+the CPU: the shard plan, and the 16-bit pair form's eligibility, unit and constants.
 
 The kernel reads each accumulator as a 16-bit value v(u) = D(u) + s*X(u) - Dmin - lo_s
 (F = D~ + 2^23 - Dlow_s in fp32, low half of the bit pattern) and adds one packed constant:
@@ -37,6 +38,8 @@ def harness(tmp_path_factory):
     L.h_tc2_u16_eligible.argtypes = [ctypes.c_int, dp, fp]
     L.h_tc2_u16_quantized.argtypes = [ctypes.c_int, dp, ctypes.c_double, dp, fp, dp]
     L.h_tc2_u16_tables.argtypes = [fp, ctypes.c_float, ctypes.POINTER(Tc2Tab)]
+    L.h_tc_plan.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                            ctypes.POINTER(ctypes.c_uint64), dp, ctypes.POINTER(ctypes.c_int)]
     assert L.h_tc2_tab_size() == ctypes.sizeof(Tc2Tab)
     return L
 
@@ -144,3 +147,43 @@ def test_exact_eligibility_needs_room_for_the_chunk_couplings(harness):
     assert fp.value == 0.0  # Dmin: no negative couplings
     W[n - 1, n - 1] = 65535.0 - 199.0  # span + offset = 2^16: refused, though the span fits
     assert harness.h_tc2_u16_eligible(n, W.ctypes.data_as(dp), ctypes.byref(fp)) == 0
+
+
+def _plan(L, n, is_int, abs_sum, idx, cnt, gl=0):
+    u = (ctypes.c_uint64 * 5)()
+    f = (ctypes.c_double * 2)()
+    i = (ctypes.c_int * 3)()
+    L.h_tc_plan(n, int(is_int), float(abs_sum), idx, cnt, gl, u, f, i)
+    return {"tile_begin": u[0], "tile_end": u[1], "rec_begin": u[2], "rec_count": u[3], "states": u[4],
+            "scale": f[0], "eps": f[1], "nt": i[0], "gl": i[1], "exact": i[2]}
+
+
+@pytest.mark.parametrize("n", [20, 21, 24, 29, 33, 36, 40])
+def test_shard_plans_partition_the_tiles_on_record_blocks(harness, n):
+    """Shards of any count (more shards than record blocks included) cover every Gray tile
+    and every record exactly once, in order, each boundary on a record block; the exact flag
+    and the digit scale follow the stated rules."""
+    for gl in (0, 5, n - 15, n - 14):  # n - 14 is out of range: the default applies
+        for cnt in (1, 2, 3, 7, 8, 64):
+            plans = [_plan(harness, n, True, 1000.0, s, cnt, gl) for s in range(cnt)]
+            g = plans[0]["gl"]
+            assert g == (gl if 5 <= gl <= n - 15 else max(5, n - 33))
+            tile, rec = 0, 0
+            for p in plans:
+                assert p["tile_begin"] == tile and p["rec_begin"] == rec
+                assert p["tile_begin"] % (1 << g) == 0 and p["tile_end"] % (1 << g) == 0
+                assert p["rec_count"] == ((p["tile_end"] - p["tile_begin"]) >> g) * 8
+                assert p["states"] == (p["tile_end"] - p["tile_begin"]) << 15
+                tile, rec = p["tile_end"], p["rec_begin"] + p["rec_count"]
+            assert tile == 1 << (n - 15) and rec == 8 << (n - 15 - g)
+            assert sum(p["states"] for p in plans) == 1 << n
+    # exact integer digits up to sum|Q| = 2^22; beyond, and for float Q, a power-of-two scale
+    # with scale * sum|Q| <= 2^14 < 2 * scale * sum|Q| and a positive error bound
+    for is_int, s in ((True, 2.0 ** 22), (True, 2.0 ** 22 + 1), (False, 3.0), (False, 12345.678), (False, 1e-3)):
+        p = _plan(harness, n, is_int, s, 0, 1)
+        exact = is_int and s <= 2.0 ** 22
+        assert p["exact"] == int(exact)
+        if exact:
+            assert p["scale"] == 1.0 and p["eps"] == 0.0
+        else:
+            assert p["scale"] * s <= 2.0 ** 14 < 2 * p["scale"] * s and p["eps"] > 0
