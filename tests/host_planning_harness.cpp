@@ -1,7 +1,7 @@
-// Host-only harness for tests/test_tc2_tables.py: exports the tensor-core forms' host-side
-// planning (the shard plan, the 16-bit pair form's eligibility, the power-of-two unit of its
-// rounded form, its per-problem table of constants) from the library's own headers so the
-// test can check them on the CPU.
+// Host-only harness for tests/test_host_planning.py: exports the tensor-core forms' host-side
+// planning (the shard plan, the record geometry, the 16-bit pair form's eligibility, the
+// power-of-two unit of its rounded form, its per-problem table of constants) from the
+// library's own headers so the test can check them on the CPU.
 // Built by the test with g++; not part of the library.
 #include "qb_tc2.cuh"
 
@@ -31,5 +31,23 @@ void h_tc_plan(int n, int is_int, double abs_sum, int shard_idx, int shard_cnt, 
   i32[1] = p.gl;
   i32[2] = p.exact ? 1 : 0;
 }
+
+// record_states of one record of a geometry: its base state and free-bit mask
+void h_record_states(int kind, int n, int a, int b, int sbits, int cbbits, int gubits, int gl, int fbits, uint64_t r,
+                     uint64_t* base, uint64_t* freem) {
+  qb::RecGeom g{};
+  g.kind = kind;
+  g.n = n;
+  g.a = a;
+  g.b = b;
+  g.sbits = sbits;
+  g.cbbits = cbbits;
+  g.gubits = gubits;
+  g.gl = gl;
+  g.fbits = fbits;
+  qb::record_states(g, r, base, freem);
+}
+
+uint64_t h_grayrank64(uint64_t g) { return qb::grayrank64(g); }
 
 }  // extern "C"

@@ -1,11 +1,12 @@
-"""Host-side planning of the tensor-core forms (csrc/qb_tc.cuh, csrc/qb_tc2.cuh), checked on
-the CPU: the shard plan, and the 16-bit pair form's eligibility, unit and constants.
+"""Host-side planning (csrc/qb_common.cuh, csrc/qb_tc.cuh, csrc/qb_tc2.cuh), checked on the
+CPU: the record geometries, the tensor-core shard plan, and the 16-bit pair form's
+eligibility, unit and constants.
 
 The kernel reads each accumulator as a 16-bit value v(u) = D(u) + s*X(u) - Dmin - lo_s
 (F = D~ + 2^23 - Dlow_s in fp32, low half of the bit pattern) and adds one packed constant:
 per chunk c = (u4, u5, u6) for tile t, giving D(u) - Dmin, and per position k = (u1, u2, u3),
 half u0 and column half u7 for the partner tile, giving D(u) + s*gamma(u) - Dmin, all modulo
-2^16.  The harness (tests/tc2_tables_harness.cpp) exports the library's own table builder
+2^16.  The harness (tests/host_planning_harness.cpp) exports the library's own table builder
 and planning functions; this test emulates the kernel's arithmetic with them."""
 import ctypes
 import os
@@ -30,9 +31,9 @@ def harness(tmp_path_factory):
     gxx = shutil.which("g++")
     if gxx is None or not os.path.isdir(CUDA_INC):
         pytest.skip("g++ or the CUDA headers are not available")
-    out = str(tmp_path_factory.mktemp("tc2") / "tc2_tables.so")
+    out = str(tmp_path_factory.mktemp("planning") / "host_planning.so")
     subprocess.run([gxx, "-std=c++17", "-O1", "-fPIC", "-shared", "-I", CSRC, "-I", CUDA_INC,
-                    os.path.join(HERE, "tc2_tables_harness.cpp"), "-o", out], check=True)
+                    os.path.join(HERE, "host_planning_harness.cpp"), "-o", out], check=True)
     L = ctypes.CDLL(out)
     dp, fp = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_float)
     L.h_tc2_u16_eligible.argtypes = [ctypes.c_int, dp, fp]
@@ -40,6 +41,10 @@ def harness(tmp_path_factory):
     L.h_tc2_u16_tables.argtypes = [fp, ctypes.c_float, ctypes.POINTER(Tc2Tab)]
     L.h_tc_plan.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                             ctypes.POINTER(ctypes.c_uint64), dp, ctypes.POINTER(ctypes.c_int)]
+    L.h_record_states.argtypes = [ctypes.c_int] * 9 + [ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+                                                      ctypes.POINTER(ctypes.c_uint64)]
+    L.h_grayrank64.argtypes = [ctypes.c_uint64]
+    L.h_grayrank64.restype = ctypes.c_uint64
     assert L.h_tc2_tab_size() == ctypes.sizeof(Tc2Tab)
     return L
 
@@ -187,3 +192,65 @@ def test_shard_plans_partition_the_tiles_on_record_blocks(harness, n):
             assert p["scale"] == 1.0 and p["eps"] == 0.0
         else:
             assert p["scale"] * s <= 2.0 ** 14 < 2 * p["scale"] * s and p["eps"] > 0
+
+
+GEOM_GRAY, GEOM_TC, GEOM_BLOCK = 1, 2, 3
+
+
+def _covered(L, geom, count):
+    """Every state of every record 0..count-1, as one array (records share one free mask)."""
+    base, free = ctypes.c_uint64(), ctypes.c_uint64()
+    bases, masks = [], set()
+    for r in range(count):
+        L.h_record_states(*geom, r, ctypes.byref(base), ctypes.byref(free))
+        bases.append(base.value)
+        masks.add(free.value)
+    assert len(masks) == 1
+    m = masks.pop()
+    pos = [i for i in range(64) if (m >> i) & 1]
+    sub = np.zeros(1 << len(pos), dtype=np.uint64)
+    for i, p in enumerate(pos):
+        sub |= ((np.arange(1 << len(pos), dtype=np.uint64) >> np.uint64(i)) & np.uint64(1)) << np.uint64(p)
+    b = np.array(bases, dtype=np.uint64)
+    assert not np.any(b & np.uint64(m))  # the base leaves the free bits clear
+    return (b[:, None] | sub[None, :]).ravel()
+
+
+def _gray_geoms(n):
+    for b in sorted({13, max(13, n - 16), n - 7}):
+        a = n - b
+        if not (7 <= a <= 24):
+            continue
+        cb = b - 13
+        for sbits in sorted({5, a, min(a, max(5, n - 34))}):
+            for ubits in sorted({max(7, sbits), a}):
+                if ubits < sbits or ubits > a:
+                    continue
+                gub = ubits - sbits
+                count = 1 << (a - ubits + cb + gub + 3)
+                yield (GEOM_GRAY, n, a, b, sbits, cb, gub, 0, 0), count
+
+
+@pytest.mark.parametrize("n", [20, 21, 22])
+def test_records_partition_the_states(harness, n):
+    """Each geometry's records, expanded to states, cover every one of the 2^n states exactly
+    once (pass 2 re-walks exactly the states of the selected records)."""
+    geoms = list(_gray_geoms(n))
+    nt = n - 15
+    for gl in sorted({5, nt}):
+        geoms.append(((GEOM_TC, n, 0, 0, 0, 0, 0, gl, 0), 8 << (nt - gl)))
+    geoms.append(((GEOM_BLOCK, n, 0, 0, 0, 0, 0, 0, min(n, 16)), 1 << (n - min(n, 16))))
+    assert len(geoms) >= 4
+    for geom, count in geoms:
+        states = _covered(harness, geom, count)
+        assert states.size == 1 << n, geom
+        assert int(states.max()) < 1 << n
+        hits = np.bincount(states.astype(np.int64), minlength=1 << n)
+        assert hits.min() == 1 and hits.max() == 1, geom
+
+
+def test_grayrank_inverts_the_gray_code(harness):
+    rng = np.random.default_rng(4)
+    for i in [0, 1, 2, 3, (1 << 63) - 1, (1 << 64) - 1] + [int(v) for v in rng.integers(0, 1 << 63, 200)]:
+        g = i ^ (i >> 1)
+        assert harness.h_grayrank64(g) == i
