@@ -1,7 +1,7 @@
-// Host-only harness for tests/test_host_planning.py: exports the tensor-core forms' host-side
-// planning (the shard plan, the record geometry, the 16-bit pair form's eligibility, the
-// power-of-two unit of its rounded form, its per-problem table of constants) from the
-// library's own headers so the test can check them on the CPU.
+// Host-only harness for tests/test_host_planning.py: exports host-side planning from the
+// library's own headers (the tensor-core shard plan, the record geometry, the tie order, the
+// 16-bit pair form's eligibility, the power-of-two unit of its rounded form and its table of
+// constants) so the test can check them on the CPU.
 // Built by the test with g++; not part of the library.
 #include "qb_tc2.cuh"
 
@@ -49,5 +49,11 @@ void h_record_states(int kind, int n, int a, int b, int sbits, int cbbits, int g
 }
 
 uint64_t h_grayrank64(uint64_t g) { return qb::grayrank64(g); }
+
+// the order key that decides ties between equal minima
+uint64_t h_tie_key(int kind, int n, int k, int A, int B, uint64_t X) {
+  const qb::TieRule r{kind, n, k, A, B};
+  return qb::tie_key(r, X);
+}
 
 }  // extern "C"

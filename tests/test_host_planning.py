@@ -1,6 +1,6 @@
 """Host-side planning (csrc/qb_common.cuh, csrc/qb_tc.cuh, csrc/qb_tc2.cuh), checked on the
-CPU: the record geometries, the tensor-core shard plan, and the 16-bit pair form's
-eligibility, unit and constants.
+CPU: the record geometries, the tie order, the tensor-core shard plan, and the 16-bit pair
+form's eligibility, unit and constants.
 
 The kernel reads each accumulator as a 16-bit value v(u) = D(u) + s*X(u) - Dmin - lo_s
 (F = D~ + 2^23 - Dlow_s in fp32, low half of the bit pattern) and adds one packed constant:
@@ -45,6 +45,8 @@ def harness(tmp_path_factory):
                                                       ctypes.POINTER(ctypes.c_uint64)]
     L.h_grayrank64.argtypes = [ctypes.c_uint64]
     L.h_grayrank64.restype = ctypes.c_uint64
+    L.h_tie_key.argtypes = [ctypes.c_int] * 5 + [ctypes.c_uint64]
+    L.h_tie_key.restype = ctypes.c_uint64
     assert L.h_tc2_tab_size() == ctypes.sizeof(Tc2Tab)
     return L
 
@@ -254,3 +256,40 @@ def test_grayrank_inverts_the_gray_code(harness):
     for i in [0, 1, 2, 3, (1 << 63) - 1, (1 << 64) - 1] + [int(v) for v in rng.integers(0, 1 << 63, 200)]:
         g = i ^ (i >> 1)
         assert harness.h_grayrank64(g) == i
+
+
+TIE_QBF, TIE_QBF1 = 0, 1
+
+
+@pytest.mark.parametrize("n,k,A", [(20, 0, 0), (24, 0, 4), (30, 0, 10), (36, 0, 16), (30, 3, 7), (36, 5, 11),
+                                   (40, 0, 20), (44, 2, 22)])
+def test_qbf_tie_order_is_the_oracles(harness, n, k, A):
+    """Sorting states by the library's tie key gives the order of the reference's prefix loop
+    (QBF: inverse-Gray rank of the prefix, then the suffix; under Parallel the task bits
+    first), as the oracle states it."""
+    import oracle
+    B = n - k - A
+    rng = np.random.default_rng(n * 100 + k)
+    xs = [int(v) for v in rng.integers(0, 1 << n, 300, dtype=np.uint64)]
+    xs += [x for x in (0, (1 << n) - 1, 1 << (n - 1), 1 << B, (1 << B) - 1) if x < 1 << n]
+    mine = sorted(xs, key=lambda x: harness.h_tie_key(TIE_QBF, n, k, A, B, x))
+    if k == 0:
+        ref = sorted(xs, key=lambda x: oracle.qbf_key(x, n, A))
+    else:
+        ref = sorted(xs, key=lambda x: oracle.parallel_key(x, n, k, A))
+    assert mine == ref
+
+
+@pytest.mark.parametrize("n,k", [(19, 0), (24, 0), (33, 0), (44, 0), (30, 2)])
+def test_qb_f1_tie_order_is_the_oracles(harness, n, k):
+    """QB_F1's answer order: task bits, then the thread of the reference kernel that owns the
+    18-bit suffix column, then the Gray step of the prefix (src/qubo_lib/solvers/qbf1.py:195-249)."""
+    import oracle
+    A = n - k - 18
+    rng = np.random.default_rng(n)
+    xs = [int(v) for v in rng.integers(0, 1 << n, 300, dtype=np.uint64)] + [0, (1 << n) - 1]
+    mine = sorted(xs, key=lambda x: harness.h_tie_key(TIE_QBF1, n, k, A, 18, x))
+    mask = (1 << 18) - 1
+    ref = sorted(xs, key=lambda x: (x >> (n - k) if k else 0, oracle.qbf1_tid(x & mask),
+                                    oracle.grayrank((x >> 18) & ((1 << A) - 1))))
+    assert mine == ref
