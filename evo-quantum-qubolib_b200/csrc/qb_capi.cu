@@ -1038,6 +1038,7 @@ int qb_solve(qb_handle* h, const qb_problem* p, const qb_options* o, qb_result* 
 
 namespace {
 
+static_assert(qb::kTcMaxGl + 12 <= qb::kExactMaxFree, "a tensor-core record must fit the exact re-walk");
 constexpr int kBatchMaxN = 36;            // larger problems are solved one by one
 constexpr int kBatchTcMinN = 24;          // from here on the tensor-core form (>= 512 tiles)
 constexpr uint64_t kBatchGtabChunk = 1024;  // G-table steps per CTA
@@ -1694,7 +1695,7 @@ int qb_autotune(qb_handle* h, int32_t n, int32_t dtype, int32_t* form_out) {
       const int gl0 = qb::tc_default_gl(n);
       for (int pair = 0; pair < 2; ++pair)
         for (int d = 0; d <= 3; ++d) {
-          if (gl0 + d > n - 15) break;
+          if (gl0 + d > std::min(n - 15, qb::kTcMaxGl)) break;
           qb_handle::Tuned t;
           t.form = QB_FORM_TC;
           t.tc_gl = gl0 + d;

@@ -159,9 +159,12 @@ inline bool tc_supported(int n) { return n >= 20 && n <= kMaxN; }
 inline double tc_error_bound(double abs_sum) { return 256.0 * abs_sum * 5.9604644775390625e-08 + 1e-300; }
 
 // default record granularity: runs of 32 tiles, at most 2^21 records (8 per block of 2^gl tiles)
-inline int tc_default_gl(int n) { return std::max(5, n - 15 - 18); }
+// largest record block: 2^28 tiles, so that a record's gl + 12 free bits (2^gl tiles x 128
+// rows x 256 columns of one block quarter and half) stay within the exact re-walk's 40
+constexpr int kTcMaxGl = 28;
+inline int tc_default_gl(int n) { return std::min(kTcMaxGl, std::max(5, n - 15 - 18)); }
 
-// gl: log2 tiles per record block (0 = tc_default_gl); 5 <= gl <= n - 15
+// gl: log2 tiles per record block (0 = tc_default_gl); 5 <= gl <= min(n - 15, kTcMaxGl)
 inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard_cnt, TcPlan* p, int gl = 0) {
   p->n = n;
   p->nt = n - 15;
@@ -177,7 +180,7 @@ inline void tc_plan(int n, bool is_int, double abs_sum, int shard_idx, int shard
     p->scale = std::ldexp(1.0, e);
     p->eps = tc_error_bound(abs_sum);
   }
-  p->gl = gl >= 5 && gl <= p->nt ? gl : tc_default_gl(n);
+  p->gl = gl >= 5 && gl <= std::min(p->nt, kTcMaxGl) ? gl : tc_default_gl(n);
   uint64_t groups = 1ull << (p->nt - p->gl);
   unsigned __int128 g = groups;
   uint64_t gb = (uint64_t)(g * (unsigned)shard_idx / (unsigned)shard_cnt);

@@ -99,7 +99,10 @@ extern "C" {
 typedef struct qb_handle_s qb_handle;
 
 typedef struct qb_problem {
-  int32_t n;            /* variables, 1..62 */
+  int32_t n;            /* variables, 1..62; one call's search must fit one launch: the
+                           tensor-core form below 2^32 tiles per CTA (n <= 54 on 148 SMs),
+                           the Gray form below 2^31 work units (n <= 59), else QB_EINVAL /
+                           QB_ECUDA -- split larger searches with shard_index/shard_count */
   int32_t dtype;        /* QB_F32 .. QB_I64 */
   const void* q;        /* n x n, row-major, leading dimension ldq elements */
   int64_t ldq;

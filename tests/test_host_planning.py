@@ -293,3 +293,20 @@ def test_qb_f1_tie_order_is_the_oracles(harness, n, k):
     ref = sorted(xs, key=lambda x: (x >> (n - k) if k else 0, oracle.qbf1_tid(x & mask),
                                     oracle.grayrank((x >> 18) & ((1 << A) - 1))))
     assert mine == ref
+
+
+EXACT_MAX_FREE = 40  # free bits of one record that the exact re-walk takes (csrc/qb_exact.cuh)
+
+
+@pytest.mark.parametrize("n", list(range(20, 63)))
+def test_tensor_core_records_stay_within_the_exact_rewalk(harness, n):
+    """Every record of the tensor-core form (2^gl tiles x 128 rows x 256 columns of a block:
+    gl + 12 free bits) must fit the exact re-walk, for the default record size and for every
+    override the plan accepts, up to the library's largest n."""
+    nt = n - 15
+    p = _plan(harness, n, True, 1000.0, 0, 1)
+    assert p["gl"] + 12 <= EXACT_MAX_FREE, p
+    for gl in range(5, nt + 2):
+        q = _plan(harness, n, True, 1000.0, 0, 1, gl)
+        assert q["gl"] + 12 <= EXACT_MAX_FREE, (gl, q)
+        assert q["gl"] == gl or q["gl"] == p["gl"]  # an accepted override, else the default
